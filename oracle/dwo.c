@@ -1,0 +1,427 @@
+/* dwo.c -- oracle: CPU restatement of deconwolf's SHB / RL iteration.
+ *
+ * TEST INFRASTRUCTURE ONLY (see dwo.h).  Each function cites the reference
+ * source it restates (paths inside the deconwolf tree).  FFTs go through
+ * oracle/cfft.c, the same code that backs the FFTW shim used to compile the
+ * reference itself into oracle/_ref, so the two agree to the order of the
+ * OpenMP reductions.
+ */
+#include "dwo.h"
+#include "cfft.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef int64_t i64;
+
+static double now_s(void)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double) t.tv_sec + 1e-9 * (double) t.tv_nsec;
+}
+
+void dwo_opts_default(dwo_opts *s)
+{
+    /* dw_opts_new, src/dw.c:340-413 (the fields the GPU path honours) */
+    memset(s, 0, sizeof(*s));
+    s->method = 2;
+    s->n_iter = 1;
+    s->iter_type = 1;
+    s->maxiter = 250;
+    s->err_rel = 0.02f;
+    s->err_abs = 1.0f;
+    s->bg = 1e-2f;
+    s->bg_auto = 1;
+    s->positivity = 1;
+    s->border_quality = 2;
+    s->start_condition = 0;
+    s->metric = 1;
+    s->alphamax = 1.0f;
+}
+
+static int nthreads(int t)
+{
+#ifdef _OPENMP
+    return t > 0 ? t : omp_get_max_threads();
+#else
+    (void) t;
+    return 1;
+#endif
+}
+
+static size_t nch(i64 M, i64 N, i64 P) { return (size_t) (1 + M / 2) * N * P; } /* fft.c:129-133 */
+
+void dwo_fft_r2c(const float *in, i64 M, i64 N, i64 P, float *out, int threads)
+{
+    /* fft.c:401-415: fftwf_plan_dft_r2c_3d(P, N, M, ...) */
+    cfft_r2c_3d(P, N, M, in, M, out, nthreads(threads));
+}
+
+void dwo_fft_c2r(float *in, i64 M, i64 N, i64 P, float *out, int threads)
+{
+    /* unnormalised inverse; fft.c:848-863 normalises afterwards */
+    cfft_c2r_3d(P, N, M, in, out, M, nthreads(threads));
+}
+
+/* fim_argmax_max, fim.c:269-332: first (lowest linear index) maximum */
+void dwo_argmax(const float *I, i64 M, i64 N, i64 P, i64 *aM, i64 *aN, i64 *aP)
+{
+    size_t MNP = (size_t) M * N * P, amax = 0;
+    float mx = I[0];
+    for (size_t k = 0; k < MNP; k++)
+        if (I[k] > mx) { mx = I[k]; amax = k; }
+    i64 p = (i64) (amax / ((size_t) M * N));
+    i64 n = (i64) ((amax - (size_t) p * M * N) / M);
+    *aP = p;
+    *aN = n;
+    *aM = (i64) amax - p * M * N - n * M;
+}
+
+static i64 mod_i64(i64 a, i64 b)
+{
+    i64 r = a % b;
+    return r < 0 ? r + b : r;
+}
+
+/* fim_circshift + shift_vector_buf, fim.c:982-1057 and 1225-1242:
+ * new[i] = old[(i - s) mod n] along each axis in turn. */
+void dwo_circshift(float *A, i64 M, i64 N, i64 P, i64 sm, i64 sn, i64 sp)
+{
+    i64 bs = M > N ? M : N;
+    bs = bs > P ? bs : P;
+    float *buf = malloc(sizeof(float) * (size_t) bs);
+    for (i64 c = 0; c < P; c++)
+        for (i64 b = 0; b < N; b++) {
+            float *v = A + b * M + c * M * N;
+            for (i64 i = 0; i < M; i++) buf[i] = v[i];
+            for (i64 i = 0; i < M; i++) v[i] = buf[mod_i64(i - sm, M)];
+        }
+    for (i64 c = 0; c < P; c++)
+        for (i64 a = 0; a < M; a++) {
+            float *v = A + a + c * M * N;
+            for (i64 i = 0; i < N; i++) buf[i] = v[i * M];
+            for (i64 i = 0; i < N; i++) v[i * M] = buf[mod_i64(i - sn, N)];
+        }
+    for (i64 b = 0; b < N; b++)
+        for (i64 a = 0; a < M; a++) {
+            float *v = A + a + b * M;
+            for (i64 i = 0; i < P; i++) buf[i] = v[i * M * N];
+            for (i64 i = 0; i < P; i++) v[i * M * N] = buf[mod_i64(i - sp, P)];
+        }
+    free(buf);
+}
+
+/* get_fIdiv, dw.c:1492-1524: mean over the image of g*logf(g/y) - (g - y)
+ * for y > 0 and g > 0; y is read with the job strides. */
+float dwo_idiv(const float *y, const float *g, i64 M, i64 N, i64 P,
+               i64 wM, i64 wN, i64 wP)
+{
+    (void) wP;
+    double I = 0;
+#pragma omp parallel for reduction(+ : I)
+    for (i64 c = 0; c < P; c++)
+        for (i64 b = 0; b < N; b++)
+            for (i64 a = 0; a < M; a++) {
+                double yv = y[a + b * wM + c * wM * wN];
+                double gv = g[a + b * M + c * M * N];
+                if (yv > 0 && gv > 0)
+                    I += gv * logf((float) (gv / yv)) - (gv - yv);
+            }
+    return (float) (I / (double) (M * N * P));
+}
+
+/* get_fMSE, dw.c:1461-1490 */
+static float dwo_mse(const float *y, const float *g, i64 M, i64 N, i64 P, i64 wM, i64 wN)
+{
+    double e = 0;
+    for (i64 c = 0; c < P; c++)
+        for (i64 b = 0; b < N; b++)
+            for (i64 a = 0; a < M; a++) {
+                double d = (double) y[a + b * wM + c * wM * wN] - (double) g[a + b * M + c * M * N];
+                e += d * d;
+            }
+    return (float) (e / (double) (M * N * P));
+}
+
+/* ------------------------------------------------------------ iterator */
+/* dw_iterator_t and dw_iterator_{new,next,set_error}, dw.h:298-306,
+ * dw.c:219-276 */
+typedef struct {
+    float error, lasterror;
+    int iter, niter;
+    float relerror, abserror;
+    int itertype;
+} dwo_it;
+
+static void it_new(dwo_it *it, const dwo_opts *s)
+{
+    it->error = 1;
+    it->lasterror = 1;
+    it->itertype = s->iter_type;
+    it->abserror = s->err_abs;
+    it->relerror = s->err_rel;
+    it->iter = -1;
+    it->niter = (s->iter_type != 2) ? s->maxiter : s->n_iter;
+}
+
+static int it_next(dwo_it *it)
+{
+    it->iter++;
+    if (it->itertype == 1) {
+        if (it->iter < 2) it->lasterror = 2 * it->error * it->relerror;
+        if (fabs(it->error - it->lasterror) / it->error < it->relerror) return -1;
+    } else if (it->itertype == 0) {
+        if (it->iter > 0 && it->error < it->abserror) return -1;
+    }
+    if (it->iter >= it->niter) return -1;
+    return it->iter;
+}
+
+static void it_set(dwo_it *it, float e)
+{
+    it->lasterror = it->error;
+    it->error = e;
+}
+
+/* ------------------------------------------------------------ helpers */
+
+typedef struct {
+    i64 M, N, P, wM, wN, wP;
+    size_t wMNP;
+    float norm;      /* divisor of the inverse transform */
+    int threads;
+    float *cbuf;     /* complex scratch, nch(w) complex */
+} job_t;
+
+/* fft_convolve_cc_f2 / fft_convolve_cc_conj_f2, fft.c:482-521: multiply the
+ * spectrum by K (or conj(K)), inverse transform, divide by the job size. */
+static void convolve(job_t *J, const float *K, float *F, int conj, float *out)
+{
+    size_t n = nch(J->wM, J->wN, J->wP);
+#pragma omp parallel for
+    for (size_t k = 0; k < n; k++) {
+        float a = K[2 * k], ac = conj ? -K[2 * k + 1] : K[2 * k + 1];
+        float b = F[2 * k], bc = F[2 * k + 1];
+        F[2 * k] = a * b - ac * bc;
+        F[2 * k + 1] = a * bc + b * ac;
+    }
+    dwo_fft_c2r(F, J->wM, J->wN, J->wP, out, J->threads);
+    float norm = J->norm;
+#pragma omp parallel for
+    for (size_t k = 0; k < J->wMNP; k++) out[k] /= norm;
+}
+
+static float get_error(job_t *J, const float *y, const float *im, int metric)
+{
+    if (metric == 0) return dwo_mse(y, im, J->M, J->N, J->P, J->wM, J->wN);
+    return dwo_idiv(y, im, J->M, J->N, J->P, J->wM, J->wN, J->wP);
+}
+
+/* ------------------------------------------------------------ driver */
+
+int dwo_deconvolve(const float *im, i64 M, i64 N, i64 P,
+                   const float *psf, i64 pM, i64 pN, i64 pP,
+                   dwo_opts *s, float *out)
+{
+    double t0 = now_s();
+    int shb = (s->method == 2);
+    size_t MNP = (size_t) M * N * P;
+    s->iterations_done = 0;
+
+    /* method_shb.c:101-105, method_rl.c:116-119 */
+    if (s->n_iter == 0) {
+        memcpy(out, im, sizeof(float) * MNP);
+        return 0;
+    }
+    if (s->start_condition == 1) return -2; /* LP start is not restated */
+
+    /* method_shb.c:108-117: bg = max(min(im), 0.01) */
+    if (s->bg_auto) {
+        float mn = im[0];
+        for (size_t k = 0; k < MNP; k++) if (im[k] < mn) mn = im[k];
+        s->bg = mn < 1e-2f ? 1e-2f : mn;
+    }
+
+    /* method_shb.c:137-153 */
+    i64 wM = M + pM - 1, wN = N + pN - 1, wP = P + pP - 1;
+    if (s->border_quality == 1) { wM = M + (pM + 1) / 2; wN = N + (pN + 1) / 2; wP = P + (pP + 1) / 2; }
+    if (s->border_quality == 0) { wM = M > pM ? M : pM; wN = N > pN ? N : pN; wP = P > pP ? P : pP; }
+    size_t wMNP_logical = (size_t) wM * wN * wP;
+    int padded = 0;
+    if (s->work[0] > 0) {
+        if (s->border_quality != 2 || s->work[0] < wM || s->work[1] < wN || s->work[2] < wP) return -1;
+        wM = s->work[0]; wN = s->work[1]; wP = s->work[2];
+        padded = 1;
+    }
+
+    job_t J;
+    J.M = M; J.N = N; J.P = P; J.wM = wM; J.wN = wN; J.wP = wP;
+    J.wMNP = (size_t) wM * wN * wP;
+    J.threads = s->threads;
+    /* ifft_inplace, fft.c:860: float MNP = (float) M*N*P (float products) */
+    J.norm = (float) wM * (float) wN * (float) wP;
+    if (padded) J.norm = (float) ((double) wM * (double) wN * (double) wP);
+    size_t wMNP = J.wMNP;
+    size_t nc = nch(wM, wN, wP);
+
+    float *K = calloc(2 * nc, sizeof(float));
+    float *C = calloc(2 * nc, sizeof(float));
+    float *Z = calloc(wMNP, sizeof(float));
+    if (!K || !C || !Z) return -3;
+
+    /* OTF, method_shb.c:185-212: insert at the corner (fim_insert,
+     * fim.c:585-623), move the argmax to the origin, transform. */
+    for (i64 c = 0; c < pP; c++)
+        for (i64 b = 0; b < pN; b++)
+            for (i64 a = 0; a < pM; a++)
+                Z[a + b * wM + c * wM * wN] = psf[a + b * pM + c * pM * pN];
+    i64 mM, mN, mP;
+    dwo_argmax(Z, wM, wN, wP, &mM, &mN, &mP);
+    dwo_circshift(Z, wM, wN, wP, -mM, -mN, -mP);
+    {
+        float mx = Z[0];
+        for (size_t k = 0; k < wMNP; k++) if (Z[k] > mx) mx = Z[k];
+        if (Z[0] != mx) { free(K); free(C); free(Z); return -4; } /* method_shb.c:199-203 */
+    }
+    dwo_fft_r2c(Z, wM, wN, wP, K, s->threads);
+
+    /* Bertero weights, method_shb.c:216-253 (initial_guess, dw.c:2497-2520) */
+    float *W = NULL;
+    if (s->border_quality > 0) {
+        memset(Z, 0, sizeof(float) * wMNP);
+        for (i64 c = 0; c < P; c++)
+            for (i64 b = 0; b < N; b++)
+                for (i64 a = 0; a < M; a++) Z[a + wM * b + wM * wN * c] = 1;
+        dwo_fft_r2c(Z, wM, wN, wP, C, s->threads);
+        W = malloc(sizeof(float) * wMNP);
+        convolve(&J, K, C, 1, W);
+        const float sigma = 0.01f;
+#pragma omp parallel for
+        for (size_t k = 0; k < wMNP; k++)
+            W[k] = (W[k] > sigma) ? (float) (1.0 / W[k]) : 0.0f;
+    }
+
+    /* fim_sum, fim.c:368-378 */
+    double sumd = 0;
+    for (size_t k = 0; k < MNP; k++) sumd += (double) im[k];
+    float sumg = (float) sumd;
+
+    float *x = malloc(sizeof(float) * wMNP);
+    float *xp = malloc(sizeof(float) * wMNP);
+    float *y = Z; /* reuse */
+    float *xn = shb ? malloc(sizeof(float) * wMNP) : NULL;
+    if (s->start_condition == 0) {
+        /* method_shb.c:264-268: sumg / wMNP with the job's voxel count */
+        float v = sumg / (float) wMNP_logical;
+        for (size_t k = 0; k < wMNP; k++) x[k] = v;
+    } else {
+        memset(x, 0, sizeof(float) * wMNP);
+        for (i64 c = 0; c < P; c++)
+            for (i64 b = 0; b < N; b++)
+                for (i64 a = 0; a < M; a++) x[a + wM * b + wM * wN * c] = im[a + M * b + M * N * c];
+    }
+    memcpy(xp, x, sizeof(float) * wMNP);
+
+    double t1 = now_s();
+    s->setup_seconds = t1 - t0;
+
+    dwo_it it;
+    it_new(&it, s);
+    while (it_next(&it) >= 0) {
+        float err;
+        if (shb) {
+            /* method_shb.c:325-339: p overwrites xp */
+            double alpha = ((float) it.iter - 1.0) / ((float) it.iter + 2.0);
+            if (alpha < 0) alpha = 0;
+            if (alpha > s->alphamax) alpha = s->alphamax;
+            float *p = xp;
+            float bg = s->bg;
+#pragma omp parallel for
+            for (size_t k = 0; k < wMNP; k++) {
+                p[k] = x[k] + alpha * (x[k] - xp[k]);
+                if (p[k] < bg) p[k] = bg;
+            }
+            /* iter_shb, method_shb.c:10-74 */
+            dwo_fft_r2c(p, wM, wN, wP, C, s->threads);
+            convolve(&J, K, C, 0, y);
+            err = get_error(&J, y, im, s->metric);
+            const double mindiv = 1e-6;
+#pragma omp parallel for
+            for (i64 cc = 0; cc < wP; cc++)
+                for (i64 bb = 0; bb < wN; bb++)
+                    for (i64 aa = 0; aa < wM; aa++) {
+                        size_t yi = aa + bb * wM + cc * wM * wN;
+                        if (aa < M && bb < N && cc < P) {
+                            if (fabs(y[yi]) < mindiv) y[yi] = copysign(mindiv, y[yi]);
+                            y[yi] = im[aa + bb * M + cc * M * N] / y[yi];
+                        } else {
+                            y[yi] = 0;
+                        }
+                    }
+            dwo_fft_r2c(y, wM, wN, wP, C, s->threads);
+            /* the new estimate goes into xp's buffer (p is consumed) */
+            convolve(&J, K, C, 1, xn);
+#pragma omp parallel for
+            for (size_t k = 0; k < wMNP; k++)
+                xn[k] *= W ? p[k] * W[k] : p[k];
+            { float *t = xp; xp = xn; xn = t; }
+            it_set(&it, err);
+            float *t = x; x = xp; xp = t; /* method_shb.c:358-363 */
+            if (s->positivity) {
+#pragma omp parallel for
+                for (size_t k = 0; k < wMNP; k++) if (x[k] < bg) x[k] = bg;
+            }
+        } else {
+            /* iter_rl, method_rl.c:28-102; f = xp is the current guess */
+            float *f = xp;
+            dwo_fft_r2c(f, wM, wN, wP, C, s->threads);
+            convolve(&J, K, C, 0, y);
+            err = get_error(&J, y, im, s->metric);
+            float bg = s->bg;
+#pragma omp parallel for
+            for (i64 cc = 0; cc < wP; cc++)
+                for (i64 bb = 0; bb < wN; bb++)
+                    for (i64 aa = 0; aa < wM; aa++) {
+                        size_t yi = aa + bb * wM + cc * wM * wN;
+                        if (aa < M && bb < N && cc < P) {
+                            y[yi] = (y[yi] > 0) ? im[aa + bb * M + cc * M * N] / y[yi] : bg;
+                        } else {
+                            y[yi] = 1e-6f;
+                        }
+                    }
+            dwo_fft_r2c(y, wM, wN, wP, C, s->threads);
+            convolve(&J, K, C, 1, x);
+#pragma omp parallel for
+            for (size_t k = 0; k < wMNP; k++)
+                x[k] *= W ? f[k] * W[k] : f[k];
+            it_set(&it, err);
+            /* method_rl.c:353-372: xp = x, clamp at bg when bg > 0 */
+            float *t = xp; xp = x; x = t;
+            if (bg > 0) {
+#pragma omp parallel for
+                for (size_t k = 0; k < wMNP; k++) if (xp[k] < bg) xp[k] = bg;
+            }
+        }
+        if (s->error_trace && it.iter < s->trace_capacity) s->error_trace[it.iter] = err;
+        s->iterations_done = it.iter + 1;
+    }
+    s->loop_seconds = now_s() - t1;
+
+    /* SHB returns the iterate before the last update (method_shb.c:385-395);
+     * RL returns the newest one (method_rl.c:393).  After the loop above,
+     * SHB's newest is x and its predecessor xp; RL's newest is xp. */
+    const float *res = xp;
+    if (shb && s->iterations_done == 0) res = x;
+    for (i64 c = 0; c < P; c++)
+        for (i64 b = 0; b < N; b++)
+            memcpy(out + b * M + c * M * N, res + b * wM + c * wM * wN, sizeof(float) * M);
+
+    free(K); free(C); free(Z); free(W); free(x); free(xp); free(xn);
+    return 0;
+}
