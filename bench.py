@@ -1,0 +1,355 @@
+"""Benchmark: SHB deconvolution of the 2048 x 2048 x 60 synthetic workload.
+
+One step = one full `dw --method shb --iter 50` deconvolution of the seeded
+synthetic 2048 x 2048 x 60 image with a 181 x 181 x 119 Born-Wolf PSF
+(lambda 670 nm): setup (background, OTF, Bertero weights, start) and 50 SHB
+iterations, on one B200 per rank.  Metric: Mvoxel*iter/s = image voxels x
+iterations / seconds, summed over ranks (weak scaling: every rank
+deconvolves its own image; no collective on the data path).
+
+  value  device-resident inputs (dwcu_deconvolve_device), CUDA events on the
+         engine's stream, max over ranks
+  e2e    the host-buffer C-ABI call dwcu_deconvolve from pinned host memory,
+         including the image/PSF upload and the result download
+  roofline  the dominant kernel class of the timed steps: algorithmic bytes
+         per launch / mean event time per launch, against the measured HBM
+         copy bandwidth (MEASURED_PEAKS.json)
+  cpu_baseline  deconwolf's own CPU SHB (oracle/_ref) on a bounded crop of
+         the same workload, extrapolated to the full job size
+
+`python bench.py --impl reference` times the reference CPU path alone (rank
+0; other ranks exit).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "shb-2048x2048x60"
+SMALL = "shb-256x256x40"
+ITERS = 50
+# generated inputs are cached between runs of one machine (kept out of git and gpurun snapshots)
+CACHE = os.environ.get("DWCU_INPUT_CACHE", os.path.join(ROOT, "_cache"))
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thr = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thr = threading.Thread(target=self._read, daemon=True)
+        self.thr.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thr:
+            self.thr.join(timeout=5)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------- reference arm
+
+def cpu_reference(im, psf, n_iter: int, crop: int):
+    """deconwolf's CPU SHB (oracle/_ref) on a crop x crop x P corner of the
+    image with the full PSF; returns seconds per iteration measured by the
+    iterator and the job voxel count of the crop."""
+    from oracle import pyoracle as po
+    sub = np.ascontiguousarray(im[:, :crop, :crop])
+    impl = "reference" if po.available("reference") else "port"
+    r = po.deconvolve(sub, psf, method="shb", n_iter=n_iter, impl=impl, threads=os.cpu_count())
+    P, N, M = sub.shape
+    pP, pN, pM = psf.shape
+    job = (M + pM - 1) * (N + pN - 1) * (P + pP - 1)
+    return r.loop_seconds / max(1, r.iterations), job, impl
+
+
+def full_job_voxels(shape, psf_shape):
+    P, N, M = shape
+    pP, pN, pM = psf_shape
+    return (M + pM - 1) * (N + pN - 1) * (P + pP - 1)
+
+
+def cpu_baseline_entry(im, psf, crop=384, iters=2):
+    per_it, job_crop, impl = cpu_reference(im, psf, iters, crop)
+    full_job = full_job_voxels(im.shape, psf.shape)
+    t_full = per_it * full_job / job_crop
+    vox = im.size
+    return {
+        "value": vox * 1e-6 / t_full, "unit": "Mvoxel*iter/s", "cores": os.cpu_count(),
+        "kind": "reference" if impl == "reference" else "port",
+        "sample": (f"{iters} SHB iterations of deconwolf's CPU method code ({impl} build, FFTW replaced by the "
+                   f"oracle FFT) on a {crop}x{crop}x{im.shape[0]} crop with the full PSF "
+                   f"(job {crop + psf.shape[2] - 1}x{crop + psf.shape[1] - 1}x{im.shape[0] + psf.shape[0] - 1}); "
+                   f"{per_it:.2f} s/iteration extrapolated per job voxel to the full job"),
+    }
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    from deconwolf_b200 import synthetic
+    im, psf = synthetic.config_inputs(WORKLOAD, CACHE)
+    crop = 384 if args.steps + args.warmup <= 12 else 256
+    from oracle import pyoracle as po
+    sub = np.ascontiguousarray(im[:, :crop, :crop])
+    impl = "reference" if po.available("reference") else "port"
+    n = args.warmup + args.steps
+    # per-iteration times from the reference's own iterator (the glue records them)
+    r = po.deconvolve(sub, psf, method="shb", n_iter=n, impl=impl, threads=os.cpu_count())
+    per_it = r.loop_seconds / max(1, r.iterations)
+    job_crop = full_job_voxels(sub.shape, psf.shape)
+    t_full = per_it * full_job_voxels(im.shape, psf.shape) / job_crop
+    value = im.size * 1e-6 / t_full
+    line = {
+        "impl": "reference", "metric": "Mvoxel*iter/s (SHB, 2048x2048x60)", "value": value,
+        "unit": "Mvoxel*iter/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_full * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "image": [2048, 2048, 60], "psf": [181, 181, 119], "method": "shb",
+                   "iterations_per_step": 1, "crop": [crop, crop, 60]},
+        "cpu_baseline": {"value": value, "unit": "Mvoxel*iter/s", "cores": os.cpu_count(),
+                         "kind": "reference" if impl == "reference" else "port",
+                         "sample": f"{n} SHB iterations (first {args.warmup} untimed in spirit; mean over all) of "
+                                   f"deconwolf's CPU method code on a {crop}x{crop}x60 crop, extrapolated per job voxel"},
+        "e2e": {"value": value, "unit": "Mvoxel*iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- B200 arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, SMALL])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warmup raised to 3 (timing rule)")
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import deconwolf_b200 as dw
+    from deconwolf_b200 import synthetic
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = local
+
+    t0 = time.time()
+    im, psf = synthetic.config_inputs(args.workload, CACHE)
+    log(f"[rank {rank}] inputs {im.shape} psf {psf.shape} in {time.time() - t0:.1f}s")
+    P, N, M = im.shape
+    work, nbytes = dw.plan_size(im.shape, psf.shape)
+
+    d_im = torch.from_numpy(im).to(f"cuda:{dev}")
+    d_psf = torch.from_numpy(psf).to(f"cuda:{dev}")
+    d_out = torch.empty_like(d_im)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        return dw.run_method_device(d_im.data_ptr(), d_psf.data_ptr(), d_out.data_ptr(), im.shape, psf.shape,
+                                    stream=stream.cuda_stream, method="shb", n_iter=ITERS, device=dev)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    dw.profile_enable(True)
+    launches0 = int(dw.lib().dwcu_launch_count())
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        res = step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = int(dw.lib().dwcu_launch_count()) - launches0
+    dw.profile_enable(False)
+    stats = dw.profile_collect()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    t_max = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    vox_it = float(im.size) * ITERS * args.steps * world
+    value = vox_it / (ms_max * 1e-3) / 1e6
+
+    # ---- end to end through the host-buffer C-ABI call
+    e2e = None
+    if not args.no_e2e:
+        h_im = torch.from_numpy(im).pin_memory()
+        h_psf = torch.from_numpy(psf).pin_memory()
+        h_out = torch.empty(im.shape, dtype=torch.float32).pin_memory()
+        o = dw.make_opts(method="shb", n_iter=ITERS, device=dev)
+
+        def e2e_step():
+            rc = dw.lib().dwcu_deconvolve(ctypes.c_void_p(h_im.data_ptr()), M, N, P, ctypes.c_void_p(h_psf.data_ptr()),
+                                          psf.shape[2], psf.shape[1], psf.shape[0], ctypes.byref(o),
+                                          ctypes.c_void_p(h_out.data_ptr()))
+            if rc:
+                raise dw.DwcuError(rc, dw.lib().dwcu_last_error().decode())
+
+        e2e_step()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        cur = torch.cuda.current_stream()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(cur)
+        torch.cuda.synchronize()
+        t_e2e = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{dev}")
+        if world > 1:
+            dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+        e2e = {"value": vox_it / (float(t_e2e.item()) * 1e-3) / 1e6, "unit": "Mvoxel*iter/s",
+               "h2d_bytes_per_step": int(im.nbytes + psf.nbytes), "d2h_bytes_per_step": int(im.nbytes)}
+
+    # ---- roofline of the dominant kernel class
+    peak, peak_kind = measured_peaks()
+    dom = max(stats, key=lambda s: s["ms"]) if stats else None
+    roof = None
+    if dom:
+        avg_s = dom["ms"] / dom["launches"] * 1e-3
+        achieved = dom["bytes_per_launch"] / avg_s / 1e9
+        roof = {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": avg_s * 1e3}
+        prof_path = os.path.join(ROOT, "profiles", "kernel_traffic.json")
+        if os.path.exists(prof_path):
+            try:
+                with open(prof_path) as f:
+                    tr = json.load(f).get(WORKLOAD if args.workload == WORKLOAD else args.workload, {})
+                roof["traffic"] = tr.get(dom["name"])
+            except Exception:
+                pass
+    kernels = sorted(
+        ({"name": s["name"], "launches": s["launches"], "ms": round(s["ms"], 3),
+          "GBps": round(s["bytes_per_launch"] * s["launches"] / (s["ms"] * 1e-3) / 1e9, 1)} for s in stats),
+        key=lambda d: -d["ms"])
+    total_k = sum(s["ms"] for s in stats) or 1.0
+
+    line = {
+        "metric": "Mvoxel*iter/s (SHB, 2048x2048x60)" if args.workload == WORKLOAD else "Mvoxel*iter/s (SHB, 256x256x40)",
+        "value": value, "unit": "Mvoxel*iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Poisson image, Born-Wolf PSF)",
+        "config": {"workload": args.workload, "image": [M, N, P], "psf": list(psf.shape[::-1]), "method": "shb",
+                   "iterations_per_step": ITERS, "job": list(work), "device_bytes_per_job": nbytes,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (~18 GB working set per step)"},
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "kernels": kernels[:8],
+        "kernel_share": {k["name"]: round(k["ms"] / total_k, 3) for k in kernels[:8]},
+        "iteration_ms": (ms_max / args.steps - res.seconds_setup * 1e3) / ITERS if res else None,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline_entry(im, psf)
+        except Exception as e:  # the checker build may be absent on a foreign machine
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

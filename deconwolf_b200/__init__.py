@@ -1,0 +1,350 @@
+"""deconwolf_b200 -- B200-native Richardson-Lucy / Scaled-Heavy-Ball deconvolution.
+
+Python host side over the C ABI in include/dwcu.h (libdwcu.so, built in this
+directory).  Two levels, mirroring deconwolf:
+
+* :func:`run_method` is the ``dw_function`` call (src/dw.h:89-91): image and
+  PSF go to the method as they are, exactly like ``s->fun(im, ..., psf, ...,
+  s)`` in dw_run (src/dw.c:2841).
+* :func:`deconvolve` mirrors the Python binding ``pydeconwolf.deconvolve``
+  (src/pywrapper/src/pydeconwolf.c:284-394), i.e. dw_run around the method:
+  the PSF is normalised to sum 1 (dw.c:2799, 2826), the offset (default 5) is
+  added to the image before the method (dw.c:2835-2838).
+
+There is no CPU path: without the built library or without a CUDA device the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = [
+    "DwcuError", "Opts", "lib", "run_method", "deconvolve", "plan_size", "Job",
+    "METHOD_RL", "METHOD_SHB", "ITER_ABS", "ITER_REL", "ITER_FIXED",
+    "START_FLAT", "START_LP", "START_IDENTITY", "METRIC_MSE", "METRIC_IDIV",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdwcu.so")
+
+METHOD_RL, METHOD_SHB = 0, 2
+ITER_ABS, ITER_REL, ITER_FIXED = 0, 1, 2
+START_FLAT, START_LP, START_IDENTITY = 0, 1, 2
+METRIC_MSE, METRIC_IDIV = 0, 1
+
+STATUS = {
+    0: "SUCCESS", 1: "INVALID_VALUE", 2: "UNSUPPORTED", 3: "OUT_OF_MEMORY", 4: "CUDA",
+    5: "INPUT", 6: "NOT_READY", 7: "CANCELLED", 8: "TIMEOUT", 9: "INTERNAL",
+}
+
+
+class DwcuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"dwcu {STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Opts(ctypes.Structure):
+    """Mirror of ``dwcu_opts`` (include/dwcu.h)."""
+
+    _fields_ = [
+        ("method", ctypes.c_int32),
+        ("n_iter", ctypes.c_int32),
+        ("iter_type", ctypes.c_int32),
+        ("maxiter", ctypes.c_int32),
+        ("err_rel", ctypes.c_float),
+        ("err_abs", ctypes.c_float),
+        ("bg", ctypes.c_float),
+        ("bg_auto", ctypes.c_int32),
+        ("positivity", ctypes.c_int32),
+        ("border_quality", ctypes.c_int32),
+        ("start_condition", ctypes.c_int32),
+        ("metric", ctypes.c_int32),
+        ("alphamax", ctypes.c_float),
+        ("device", ctypes.c_int32),
+        ("verbosity", ctypes.c_int32),
+        ("use_graph", ctypes.c_int32),
+        ("iterations_done", ctypes.c_int32),
+        ("error_trace", ctypes.POINTER(ctypes.c_float)),
+        ("trace_capacity", ctypes.c_int32),
+        ("work", ctypes.c_int64 * 3),
+        ("seconds_setup", ctypes.c_double),
+        ("seconds_iterate", ctypes.c_double),
+    ]
+
+
+class KernelStat(ctypes.Structure):
+    """Mirror of ``dwcu_kernel_stat``."""
+
+    _fields_ = [("name", ctypes.c_char * 40), ("launches", ctypes.c_int64),
+                ("milliseconds", ctypes.c_double), ("bytes_per_launch", ctypes.c_double)]
+
+
+def profile_enable(on: bool = True) -> None:
+    _check(lib().dwcu_profile_enable(1 if on else 0))
+
+
+def profile_collect() -> list[dict]:
+    """Per-kernel-class launches, summed event milliseconds and algorithmic
+    bytes per launch since the last collect (waits for the recorded work)."""
+    cap = 256
+    arr = (KernelStat * cap)()
+    n = ctypes.c_int32()
+    _check(lib().dwcu_profile_collect(arr, cap, ctypes.byref(n)))
+    return [dict(name=arr[i].name.decode(), launches=int(arr[i].launches), ms=float(arr[i].milliseconds),
+                 bytes_per_launch=float(arr[i].bytes_per_launch)) for i in range(min(n.value, cap))]
+
+
+# every symbol include/dwcu.h declares
+EXPORTS = [
+    "dwcu_opts_init", "dwcu_deconvolve", "dwcu_deconvolve_device", "dwcu_plan_size",
+    "dwcu_job_create", "dwcu_job_setup", "dwcu_job_step", "dwcu_job_done", "dwcu_job_result",
+    "dwcu_job_destroy", "dwcu_job_set_stream", "dwcu_job_bytes", "dwcu_last_error",
+    "dwcu_abi_version", "dwcu_device_count", "dwcu_launch_count", "dwcu_fft_r2c", "dwcu_fft_c2r",
+    "dwcu_profile_enable", "dwcu_profile_collect",
+]
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libdwcu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {HERE}/csrc -j8` "
+                          "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    i64, i32, vp = ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p
+    P_opts = ctypes.POINTER(Opts)
+    L.dwcu_opts_init.argtypes = [P_opts]
+    L.dwcu_opts_init.restype = None
+    L.dwcu_deconvolve.argtypes = [vp, i64, i64, i64, vp, i64, i64, i64, P_opts, vp]
+    L.dwcu_deconvolve.restype = ctypes.c_int
+    L.dwcu_deconvolve_device.argtypes = [vp, i64, i64, i64, vp, i64, i64, i64, P_opts, vp, vp]
+    L.dwcu_deconvolve_device.restype = ctypes.c_int
+    L.dwcu_plan_size.argtypes = [i64, i64, i64, i64, i64, i64, i32, i32, ctypes.POINTER(i64), ctypes.POINTER(i64)]
+    L.dwcu_plan_size.restype = ctypes.c_int
+    L.dwcu_job_create.argtypes = [i64, i64, i64, i64, i64, i64, P_opts, ctypes.POINTER(vp)]
+    L.dwcu_job_create.restype = ctypes.c_int
+    L.dwcu_job_setup.argtypes = [vp, vp, vp, i32]
+    L.dwcu_job_setup.restype = ctypes.c_int
+    L.dwcu_job_step.argtypes = [vp, i32, ctypes.POINTER(i32)]
+    L.dwcu_job_step.restype = ctypes.c_int
+    L.dwcu_job_done.argtypes = [vp]
+    L.dwcu_job_done.restype = ctypes.c_int
+    L.dwcu_job_result.argtypes = [vp, vp, i32, P_opts]
+    L.dwcu_job_result.restype = ctypes.c_int
+    L.dwcu_job_destroy.argtypes = [vp]
+    L.dwcu_job_destroy.restype = None
+    L.dwcu_job_set_stream.argtypes = [vp, vp]
+    L.dwcu_job_set_stream.restype = ctypes.c_int
+    L.dwcu_job_bytes.argtypes = [vp]
+    L.dwcu_job_bytes.restype = i64
+    L.dwcu_last_error.argtypes = []
+    L.dwcu_last_error.restype = ctypes.c_char_p
+    L.dwcu_abi_version.restype = ctypes.c_int
+    L.dwcu_device_count.restype = ctypes.c_int
+    L.dwcu_launch_count.restype = i64
+    L.dwcu_profile_enable.argtypes = [i32]
+    L.dwcu_profile_enable.restype = ctypes.c_int
+    L.dwcu_profile_collect.argtypes = [ctypes.POINTER(KernelStat), i32, ctypes.POINTER(i32)]
+    L.dwcu_profile_collect.restype = ctypes.c_int
+    for fn in (L.dwcu_fft_r2c, L.dwcu_fft_c2r):
+        fn.argtypes = [vp, i64, i64, i64, vp, i32, vp]
+        fn.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise DwcuError(rc, lib().dwcu_last_error().decode(errors="replace"))
+
+
+def make_opts(*, method: str | int = "shb", n_iter: int = 50, iter_type: int = ITER_FIXED,
+              maxiter: int = 250, err_rel: float = 0.02, err_abs: float = 1.0,
+              bg: float | None = None, positivity: bool = True, border_quality: int = 2,
+              start: int = START_FLAT, metric: int = METRIC_IDIV, alphamax: float = 1.0,
+              device: int = 0, verbosity: int = 0, use_graph: bool = True) -> Opts:
+    o = Opts()
+    lib().dwcu_opts_init(ctypes.byref(o))
+    if isinstance(method, str):
+        method = {"shb": METHOD_SHB, "rl": METHOD_RL}[method.lower()]
+    o.method = method
+    o.n_iter = n_iter
+    o.iter_type = iter_type
+    o.maxiter = maxiter
+    o.err_rel = err_rel
+    o.err_abs = err_abs
+    o.bg_auto = 1 if bg is None else 0
+    o.bg = 0.01 if bg is None else bg
+    o.positivity = 1 if positivity else 0
+    o.border_quality = border_quality
+    o.start_condition = start
+    o.metric = metric
+    o.alphamax = alphamax
+    o.device = device
+    o.verbosity = verbosity
+    o.use_graph = 1 if use_graph else 0
+    return o
+
+
+class Result:
+    def __init__(self, out, trace, o: Opts):
+        self.out = out
+        self.trace = trace
+        self.iterations = o.iterations_done
+        self.bg = o.bg
+        self.work = tuple(o.work)
+        self.seconds_setup = o.seconds_setup
+        self.seconds_iterate = o.seconds_iterate
+
+
+def run_method(im: np.ndarray, psf: np.ndarray, **kw) -> Result:
+    """The dw_function call on host arrays: ``im`` (P, N, M) and ``psf``
+    (pP, pN, pM), float32, x fastest.  Keyword options as :func:`make_opts`."""
+    im = np.ascontiguousarray(im, dtype=np.float32)
+    psf = np.ascontiguousarray(psf, dtype=np.float32)
+    if im.ndim != 3 or psf.ndim != 3:
+        raise ValueError("image and PSF must be 3-D (P, N, M) arrays")
+    o = make_opts(**kw)
+    cap = max(o.n_iter, o.maxiter, 1)
+    trace = np.zeros(cap, dtype=np.float32)
+    o.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    o.trace_capacity = cap
+    out = np.empty_like(im)
+    P, N, M = im.shape
+    pP, pN, pM = psf.shape
+    _check(lib().dwcu_deconvolve(im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP,
+                                 ctypes.byref(o), out.ctypes.data))
+    return Result(out, trace[: o.iterations_done].copy(), o)
+
+
+def run_method_device(d_im, d_psf, d_out, shape, psf_shape, stream: int = 0, **kw) -> Result:
+    """The dw_function call on device buffers (raw device pointers, e.g.
+    ``tensor.data_ptr()``); ``stream`` is a cudaStream_t handle or 0."""
+    o = make_opts(**kw)
+    cap = max(o.n_iter, o.maxiter, 1)
+    trace = np.zeros(cap, dtype=np.float32)
+    o.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    o.trace_capacity = cap
+    P, N, M = shape
+    pP, pN, pM = psf_shape
+    _check(lib().dwcu_deconvolve_device(ctypes.c_void_p(d_im), M, N, P, ctypes.c_void_p(d_psf), pM, pN, pP,
+                                        ctypes.byref(o), ctypes.c_void_p(d_out), ctypes.c_void_p(stream or None)))
+    return Result(None, trace[: o.iterations_done].copy(), o)
+
+
+def fft_r2c_device(d_in: int, shape, d_out: int, device: int = 0, stream: int = 0) -> None:
+    """3-D R2C (fft() of src/fft.c:401-415) on device buffers; shape (P, N, M)."""
+    P, N, M = shape
+    _check(lib().dwcu_fft_r2c(ctypes.c_void_p(d_in), M, N, P, ctypes.c_void_p(d_out), device,
+                              ctypes.c_void_p(stream or None)))
+
+
+def fft_c2r_device(d_in: int, shape, d_out: int, device: int = 0, stream: int = 0) -> None:
+    """Unnormalised 3-D C2R on device buffers; shape (P, N, M) of the real output."""
+    P, N, M = shape
+    _check(lib().dwcu_fft_c2r(ctypes.c_void_p(d_in), M, N, P, ctypes.c_void_p(d_out), device,
+                              ctypes.c_void_p(stream or None)))
+
+
+def plan_size(shape, psf_shape, border_quality: int = 2, method: str = "shb"):
+    """Padded job size (X, Y, Z) and device bytes for a job."""
+    P, N, M = shape
+    pP, pN, pM = psf_shape
+    work = (ctypes.c_int64 * 3)()
+    nbytes = ctypes.c_int64()
+    _check(lib().dwcu_plan_size(M, N, P, pM, pN, pP, border_quality,
+                                METHOD_SHB if method == "shb" else METHOD_RL, work, ctypes.byref(nbytes)))
+    return tuple(work), nbytes.value
+
+
+class Job:
+    """A resident deconvolution job (dwcu_job_*): setup once, step, read."""
+
+    def __init__(self, shape, psf_shape, **kw):
+        self.shape = tuple(shape)
+        self.psf_shape = tuple(psf_shape)
+        self.opts = make_opts(**kw)
+        P, N, M = self.shape
+        pP, pN, pM = self.psf_shape
+        h = ctypes.c_void_p()
+        _check(lib().dwcu_job_create(M, N, P, pM, pN, pP, ctypes.byref(self.opts), ctypes.byref(h)))
+        self.h = h
+
+    def setup(self, im, psf, on_device: bool = False):
+        if on_device:
+            _check(lib().dwcu_job_setup(self.h, ctypes.c_void_p(im), ctypes.c_void_p(psf), 1))
+        else:
+            self._im = np.ascontiguousarray(im, dtype=np.float32)
+            self._psf = np.ascontiguousarray(psf, dtype=np.float32)
+            _check(lib().dwcu_job_setup(self.h, self._im.ctypes.data, self._psf.ctypes.data, 0))
+
+    def step(self, n: int) -> int:
+        rem = ctypes.c_int32()
+        _check(lib().dwcu_job_step(self.h, n, ctypes.byref(rem)))
+        return rem.value
+
+    def done(self) -> bool:
+        return bool(lib().dwcu_job_done(self.h))
+
+    def set_stream(self, stream: int) -> None:
+        _check(lib().dwcu_job_set_stream(self.h, ctypes.c_void_p(stream or None)))
+
+    def nbytes(self) -> int:
+        return int(lib().dwcu_job_bytes(self.h))
+
+    def result(self, out=None, on_device: bool = False) -> Result:
+        o = Opts()
+        lib().dwcu_opts_init(ctypes.byref(o))
+        cap = max(self.opts.n_iter, self.opts.maxiter, 1)
+        trace = np.zeros(cap, dtype=np.float32)
+        o.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        o.trace_capacity = cap
+        if on_device:
+            _check(lib().dwcu_job_result(self.h, ctypes.c_void_p(out), 1, ctypes.byref(o)))
+            return Result(None, trace[: o.iterations_done].copy(), o)
+        arr = np.empty(self.shape, dtype=np.float32) if out is None else out
+        _check(lib().dwcu_job_result(self.h, arr.ctypes.data, 0, ctypes.byref(o)))
+        return Result(arr, trace[: o.iterations_done].copy(), o)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().dwcu_job_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def deconvolve(image: np.ndarray, psf: np.ndarray, iterations: int, bq: int = 2, verbose: int = 0,
+               threads: int | None = None, gpu: bool = True, *, method: str = "shb",
+               offset: float = 5.0, device: int = 0) -> np.ndarray:
+    """pydeconwolf.deconvolve(image, psf, iterations, bq, verbose, threads,
+    gpu) (pydeconwolf.c:284-394): fixed iteration count, PSF normalised to
+    sum 1 (dw.c:2799), offset added before the method (dw.c:2835-2838).
+    ``threads`` is accepted for signature compatibility (the work runs on
+    the GPU); ``gpu=False`` is rejected: this package has no CPU path."""
+    if not gpu:
+        raise ValueError("deconwolf_b200 runs on the GPU only (gpu=False is not available)")
+    im = np.array(image, dtype=np.float32, copy=True)
+    if np.min(im) < 0:
+        raise ValueError("The image contains negative values, can not continue!")  # dw.c:2703-2710
+    if np.max(im) < 1.0:
+        raise ValueError("The image has too low intensity, can not continue!")  # dw.c:2711-2721
+    p = np.array(psf, dtype=np.float32, copy=True)
+    p /= np.float32(p.sum(dtype=np.float64))
+    if offset > 0:
+        im += np.float32(offset)
+    res = run_method(im, p, method=method, n_iter=iterations, iter_type=ITER_FIXED,
+                     border_quality=bq, verbosity=verbose, device=device)
+    return res.out

@@ -1,0 +1,1086 @@
+// engine.cu -- host side of the engine: plans, jobs, iteration schedule, C ABI.
+//
+// One job = one image deconvolution with all of its state resident in HBM:
+//   g    image (pitched rows)                G bytes
+//   S    working half-spectrum                C bytes
+//   K    OTF (scaled by 1/(X*Y*Z))            C bytes
+//   xa   estimate x_k                         R bytes
+//   xb   previous estimate x_{k-1} (SHB)      R bytes
+//   W    Bertero weights (bq > 0)             R bytes
+// plus the per-iteration error partials and trace.  One SHB iteration is
+//   y-fwd, z-conv(K), y-inv, x[C2R -> I-div -> ratio -> R2C],
+//   y-fwd, z-conv(conj K), y-inv, x[C2R -> update -> next extrapolation -> R2C]
+// i.e. 8 passes over the spectrum and one read/write of the estimates.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dwcu.h"
+#include "misc_kernels.cuh"
+#include "plans_gen.h"
+
+namespace dwcu {
+
+// ------------------------------------------------------------ errors
+
+static thread_local std::string g_last_error;
+static thread_local long long g_launches = 0;
+
+static int fail(int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CU(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(e_ == cudaErrorMemoryAllocation ? DWCU_ERROR_OUT_OF_MEMORY : DWCU_ERROR_CUDA, \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define CHECK_LAUNCH()                                                                        \
+    do {                                                                                      \
+        ++g_launches;                                                                         \
+        cudaError_t e_ = cudaGetLastError();                                                  \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(DWCU_ERROR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                  \
+    } while (0)
+
+// ------------------------------------------------------------ profiling
+
+struct ProfRec {
+    int cls;
+    cudaEvent_t a, b;
+};
+struct ProfClass {
+    std::string name;
+    double bytes;
+};
+static std::mutex g_prof_mu;
+static bool g_prof_on = false;
+static std::vector<ProfRec> g_prof_recs;
+static std::vector<cudaEvent_t> g_prof_pool;
+static std::vector<ProfClass> g_prof_classes;
+
+static int prof_class(const char *name, double bytes)
+{
+    for (size_t i = 0; i < g_prof_classes.size(); ++i)
+        if (g_prof_classes[i].name == name && g_prof_classes[i].bytes == bytes) return (int) i;
+    g_prof_classes.push_back({name, bytes});
+    return (int) g_prof_classes.size() - 1;
+}
+
+static cudaEvent_t prof_event()
+{
+    if (!g_prof_pool.empty()) {
+        cudaEvent_t e = g_prof_pool.back();
+        g_prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// bracket one launch: call with begin=true before and begin=false after
+struct ProfScope {
+    bool on = false;
+    ProfRec rec{};
+    cudaStream_t st = nullptr;
+    ProfScope(const char *name, double bytes, cudaStream_t s)
+    {
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        if (!g_prof_on) return;
+        on = true;
+        st = s;
+        rec.cls = prof_class(name, bytes);
+        rec.a = prof_event();
+        rec.b = prof_event();
+        cudaEventRecord(rec.a, st);
+    }
+    ~ProfScope()
+    {
+        if (!on) return;
+        cudaEventRecord(rec.b, st);
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        g_prof_recs.push_back(rec);
+    }
+};
+
+// ------------------------------------------------------------ plans
+
+static const LinesPlan *find_lines(int n)
+{
+    for (const auto &p : kLinesPlans)
+        if (p.n == n) return &p;
+    return nullptr;
+}
+static const XPlan *find_x(int n)
+{
+    for (const auto &p : kXPlans)
+        if (p.n == n) return &p;
+    return nullptr;
+}
+
+// smallest supported length >= w (exact: only w itself)
+static long long pad_lines(long long w, bool exact)
+{
+    if (w == 1) return 1;
+    if (exact) return find_lines((int) w) ? w : -1;
+    for (const auto &p : kLinesPlans)
+        if (p.n >= w) return p.n;
+    return -1;
+}
+static long long pad_x(long long w, bool exact)
+{
+    // X even with X/2 supported by the x pass
+    if (exact) return (w % 2 == 0 && find_x((int) (w / 2))) ? w : -1;
+    for (const auto &p : kXPlans)
+        if (2LL * p.n >= w) return 2LL * p.n;
+    return -1;
+}
+
+struct Geometry {
+    long long M, N, P, pM, pN, pP;
+    long long wM, wN, wP;   // the reference's job size (method_shb.c:137-153)
+    long long X, Y, Z;      // padded job size
+    long long XC;           // complex row pitch
+    long long GP;           // image row pitch
+    const XPlan *xp;
+    const LinesPlan *yp, *zp;
+};
+
+static int make_geometry(long long M, long long N, long long P, long long pM, long long pN, long long pP, int bq,
+                         Geometry &g)
+{
+    if (M < 1 || N < 1 || P < 1 || pM < 1 || pN < 1 || pP < 1)
+        return fail(DWCU_ERROR_INVALID_VALUE, "image and PSF sizes must be positive");
+    g.M = M; g.N = N; g.P = P; g.pM = pM; g.pN = pN; g.pP = pP;
+    if (bq == 2) {
+        g.wM = M + pM - 1; g.wN = N + pN - 1; g.wP = P + pP - 1;
+    } else if (bq == 1) {
+        g.wM = M + (pM + 1) / 2; g.wN = N + (pN + 1) / 2; g.wP = P + (pP + 1) / 2;
+    } else if (bq == 0) {
+        g.wM = std::max(M, pM); g.wN = std::max(N, pN); g.wP = std::max(P, pP);
+    } else {
+        return fail(DWCU_ERROR_INVALID_VALUE, "border_quality must be 0, 1 or 2 (got %d)", bq);
+    }
+    // Only bq = 2 leaves room for the whole PSF around the image, so only then
+    // is a larger (padded) transform size mathematically identical to the
+    // reference's job size; bq 0 and 1 wrap around and need the exact size.
+    const bool exact = (bq != 2);
+    g.X = pad_x(g.wM, exact);
+    g.Y = pad_lines(g.wN, exact);
+    g.Z = pad_lines(g.wP, exact);
+    if (g.X < 0 || g.Y < 0 || g.Z < 0)
+        return fail(DWCU_ERROR_UNSUPPORTED,
+                    "no supported FFT size for job %lld x %lld x %lld (border_quality %d needs exact "
+                    "7-smooth sizes with three radices <= 16; x must be even)",
+                    g.wM, g.wN, g.wP, bq);
+    g.xp = find_x((int) (g.X / 2));
+    g.yp = g.Y > 1 ? find_lines((int) g.Y) : nullptr;
+    g.zp = g.Z > 1 ? find_lines((int) g.Z) : nullptr;
+    if (!g.xp) return fail(DWCU_ERROR_UNSUPPORTED, "x length %lld unsupported", g.X);
+    g.XC = (g.X / 2 + 1 + 1) & ~1LL;
+    g.GP = (M + 1) & ~1LL;
+    return DWCU_SUCCESS;
+}
+
+static long long x_blocks(const Geometry &g) { return (g.Y * g.Z + g.xp->R - 1) / g.xp->R; }
+
+// ------------------------------------------------------------ twiddles
+
+struct DeviceCtx {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    std::map<long long, float2 *> tw;  // length -> exp(-2 pi i m / length)
+};
+
+static std::mutex g_ctx_mu;
+static std::map<int, DeviceCtx *> g_ctx;
+
+static int get_ctx(int device, DeviceCtx **out)
+{
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = g_ctx.find(device);
+    if (it != g_ctx.end()) {
+        *out = it->second;
+        return DWCU_SUCCESS;
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(DWCU_ERROR_CUDA, "no CUDA device available (the engine has no CPU path)");
+    }
+    if (device < 0 || device >= n) return fail(DWCU_ERROR_INVALID_VALUE, "device %d out of range (%d)", device, n);
+    CU(cudaSetDevice(device));
+    auto *c = new DeviceCtx();
+    c->device = device;
+    CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    g_ctx[device] = c;
+    *out = c;
+    return DWCU_SUCCESS;
+}
+
+// twiddle table of a length, evaluated in double from the exact angle
+// reduction in dft.cuh and rounded once to float
+static int get_twiddles(DeviceCtx *c, long long n, const float2 **out)
+{
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = c->tw.find(n);
+    if (it != c->tw.end()) {
+        *out = it->second;
+        return DWCU_SUCCESS;
+    }
+    std::vector<float2> h((size_t) n);
+    for (long long m = 0; m < n; ++m)
+        h[(size_t) m] = make_float2((float) cx::cospi_frac(2 * m, n), (float) -cx::sinpi_frac(2 * m, n));
+    float2 *d = nullptr;
+    CU(cudaMalloc(&d, sizeof(float2) * (size_t) n));
+    CU(cudaMemcpy(d, h.data(), sizeof(float2) * (size_t) n, cudaMemcpyHostToDevice));
+    c->tw[n] = d;
+    *out = d;
+    return DWCU_SUCCESS;
+}
+
+// ------------------------------------------------------------ host iterator
+
+// dw_iterator_t and dw_iterator_{new,next,set_error} (src/dw.h:298-306,
+// src/dw.c:219-276)
+struct Iter {
+    float error = 1, lasterror = 1;
+    int iter = -1, niter = 0;
+    float relerror = 0, abserror = 0;
+    int itertype = DWCU_ITER_FIXED;
+    void init(const dwcu_opts &s)
+    {
+        error = 1; lasterror = 1;
+        itertype = s.iter_type;
+        abserror = s.err_abs;
+        relerror = s.err_rel;
+        iter = -1;
+        niter = (s.iter_type != DWCU_ITER_FIXED) ? s.maxiter : s.n_iter;
+    }
+    int next()
+    {
+        iter++;
+        if (itertype == DWCU_ITER_REL) {
+            if (iter < 2) lasterror = 2 * error * relerror;
+            if (std::fabs(error - lasterror) / error < relerror) return -1;
+        } else if (itertype == DWCU_ITER_ABS) {
+            if (iter > 0 && error < abserror) return -1;
+        }
+        if (iter >= niter) return -1;
+        return iter;
+    }
+    void set(float e)
+    {
+        lasterror = error;
+        error = e;
+    }
+};
+
+// ------------------------------------------------------------ the job
+
+static inline size_t align256(size_t v) { return (v + 255) & ~(size_t) 255; }
+
+}  // namespace dwcu
+
+struct dwcu_job {
+    dwcu_opts s;
+    dwcu::Geometry g;
+    dwcu::DeviceCtx *ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    // device memory
+    char *base = nullptr;
+    size_t bytes = 0;
+    float *gimg = nullptr;
+    float2 *S = nullptr, *K = nullptr;
+    float *xa = nullptr, *xb = nullptr, *W = nullptr;
+    double *partial = nullptr;
+    dwcu::JobScalars *sc = nullptr;
+    float *err = nullptr;          // device error trace
+    long long *amax = nullptr;
+    dwcu::StatsPartial *spart = nullptr;
+    dwcu::ArgmaxPartial *apart = nullptr;
+    float *psf_dev = nullptr;      // staging for the PSF
+    int n_spart = 0, n_apart = 0;
+    long long nxb = 0;             // x-pass blocks (= error partials)
+    const float2 *tw_x = nullptr, *tw_l = nullptr, *tw_y = nullptr, *tw_z = nullptr;
+    // iteration state
+    dwcu::Iter it;
+    int k_next = -1;               // iteration whose forward half runs next; -1: finished
+    bool spectrum_ready = false;   // S holds the transform of iteration k_next's input
+    int done_iters = 0;
+    bool finished = false;
+    bool setup_done = false;
+    float *h_err = nullptr;        // pinned readback slot
+    std::vector<float> trace;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    bool loop_started = false;
+    cudaGraphExec_t graph = nullptr;
+};
+
+namespace dwcu {
+
+static int trace_cap(const dwcu_opts &s) { return std::max(1, std::max(s.n_iter, s.maxiter)); }
+
+// ---- pass launchers
+
+static int launch_lines(dwcu_job *j, const LinesPlan *p, const float2 *tw, long long n, long long line_stride,
+                        long long outer_stride, long long nouter, long long ncols, int mode, float2 *data,
+                        const char *axis)
+{
+    if (!p) return DWCU_SUCCESS;  // length-1 axis: identity
+    LinesArgs a;
+    a.data = data;
+    a.otf = j->K;
+    a.tw = tw;
+    a.line_stride = line_stride;
+    a.outer_stride = outer_stride;
+    a.ncols = (int) ncols;
+    a.ntiles = (int) ((ncols + p->T - 1) / p->T);
+    a.mode = mode;
+    long long nb = (long long) a.ntiles * nouter;
+    if (nb > 0x7fffffffLL) return fail(DWCU_ERROR_UNSUPPORTED, "grid too large");
+    static const char *names[] = {"lines_fwd", "lines_inv", "lines_conv", "lines_conv_conj"};
+    char nm[40];
+    snprintf(nm, sizeof nm, "%s_%s", names[mode], axis);
+    const double elems = (double) ncols * (double) nouter * (double) n;
+    ProfScope ps(nm, elems * 8.0 * (mode >= LINES_CONV ? 3.0 : 2.0), j->stream);
+    p->launch(a, (int) nb, j->stream);
+    CHECK_LAUNCH();
+    return DWCU_SUCCESS;
+}
+
+static int pass_y(dwcu_job *j, int mode, float2 *data)
+{
+    const Geometry &g = j->g;
+    // lines along y: stride XC, outer = z planes, columns = X/2+1
+    return launch_lines(j, g.yp, j->tw_y, g.Y, g.XC, g.XC * g.Y, g.Z, g.X / 2 + 1, mode, data, "y");
+}
+static int pass_z(dwcu_job *j, int mode, float2 *data)
+{
+    const Geometry &g = j->g;
+    // lines along z: stride XC*Y, outer = y rows, columns = X/2+1
+    return launch_lines(j, g.zp, j->tw_z, g.Z, g.XC * g.Y, g.XC, g.Y, g.X / 2 + 1, mode, data, "z");
+}
+
+static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, const float *srcp, float *dst,
+                  double alpha, double alpha_next)
+{
+    const Geometry &g = j->g;
+    XArgs a;
+    a.S = S;
+    a.tw = j->tw_x;
+    a.twL = j->tw_l;
+    a.g = j->gimg;
+    a.src = src;
+    a.srcp = srcp;
+    a.Wt = j->W;
+    a.dst = dst;
+    a.partial = j->partial;
+    a.sc = j->sc;
+    a.XC = g.XC;
+    a.X = g.X;
+    a.GP = g.GP;
+    a.Y = (int) g.Y;
+    a.Z = (int) g.Z;
+    a.M = (int) g.M;
+    a.N = (int) g.N;
+    a.P = (int) g.P;
+    a.nrows = (int) (g.Y * g.Z);
+    a.op = op;
+    a.r2c = r2c;
+    a.metric = j->s.metric;
+    a.positivity = j->s.positivity;
+    a.rl_clamp = 1;
+    a.alpha = alpha;
+    a.alpha_next = alpha_next;
+    // algorithmic traffic of this launch
+    static const char *names[] = {"x_fwd_copy", "x_fwd_ones", "x_fwd_shbp", "x_ratio_shb", "x_ratio_rl",
+                                  "x_error", "x_update_shb", "x_update_rl", "x_weights", "x_store"};
+    const double C = 8.0 * (double) (g.X / 2 + 1) * (double) (g.Y * g.Z);
+    const double R = 4.0 * (double) g.X * (double) (g.Y * g.Z);
+    const double G = 4.0 * (double) (g.M * g.N * g.P);
+    static const double real_in[] = {1, 0, 2, 0, 0, 0, 3, 2, 0, 0};
+    static const double real_out[] = {0, 0, 0, 0, 0, 0, 1, 1, 1, 1};
+    double bytes = (op >= XOP_RATIO_SHB ? C : 0.0) + (r2c ? C : 0.0) + (real_in[op] + real_out[op]) * R;
+    if (op == XOP_UPDATE_SHB && !j->W) bytes -= R;
+    if (op == XOP_UPDATE_RL && !j->W) bytes -= R;
+    if (op == XOP_RATIO_SHB || op == XOP_RATIO_RL || op == XOP_ERROR_ONLY) bytes += G;
+    ProfScope ps(names[op], bytes, j->stream);
+    g.xp->launch(a, (int) j->nxb, j->stream);
+    CHECK_LAUNCH();
+    return DWCU_SUCCESS;
+}
+
+static int err_final(dwcu_job *j, int k)
+{
+    const Geometry &g = j->g;
+    k_err_final<<<1, kRedThreads, 0, j->stream>>>(j->partial, (int) j->nxb, (double) (g.M * g.N * g.P), j->err + k);
+    CHECK_LAUNCH();
+    return DWCU_SUCCESS;
+}
+
+#define TRY(x)                          \
+    do {                                \
+        int rc_ = (x);                  \
+        if (rc_ != DWCU_SUCCESS) return rc_; \
+    } while (0)
+
+// method_shb.c:328-330: alpha = clamp((k - 1)/(k + 2), 0, alphamax)
+static double shb_alpha(int k, float alphamax)
+{
+    double a = ((float) k - 1.0) / ((float) k + 2.0);
+    if (a < 0) a = 0;
+    if (a > alphamax) a = alphamax;
+    return a;
+}
+
+static int conv(dwcu_job *j, int conj)
+{
+    TRY(pass_y(j, LINES_FWD, j->S));
+    TRY(pass_z(j, conj ? LINES_CONV_CONJ : LINES_CONV, j->S));
+    TRY(pass_y(j, LINES_INV, j->S));
+    return DWCU_SUCCESS;
+}
+
+// forward half of iteration k: y = K p_k, error_k; when `ratio`, also the
+// ratio's transform into S
+static int iter_forward(dwcu_job *j, int k, bool ratio)
+{
+    const bool shb = (j->s.method == DWCU_METHOD_SHB);
+    TRY(conv(j, 0));
+    int op = ratio ? (shb ? XOP_RATIO_SHB : XOP_RATIO_RL) : XOP_ERROR_ONLY;
+    TRY(pass_x(j, op, ratio ? 1 : 0, j->S, nullptr, nullptr, nullptr, 0, 0));
+    TRY(err_final(j, k));
+    return DWCU_SUCCESS;
+}
+
+// back-projection half of iteration k: x_{k+1}; with `next`, also the
+// transform of the next iteration's input into S
+static int iter_backward(dwcu_job *j, int k, bool next)
+{
+    const bool shb = (j->s.method == DWCU_METHOD_SHB);
+    TRY(conv(j, 1));
+    if (shb) {
+        TRY(pass_x(j, XOP_UPDATE_SHB, next ? 1 : 0, j->S, j->xa, j->xb, j->xb, shb_alpha(k, j->s.alphamax),
+                   shb_alpha(k + 1, j->s.alphamax)));
+        std::swap(j->xa, j->xb);  // xa = x_{k+1}, xb = x_k
+    } else {
+        TRY(pass_x(j, XOP_UPDATE_RL, next ? 1 : 0, j->S, j->xa, nullptr, j->xa, 0, 0));
+    }
+    return DWCU_SUCCESS;
+}
+
+// transform of iteration k's input (p_k for SHB, x_k for RL) into S
+static int iter_input(dwcu_job *j, int k)
+{
+    if (j->s.method == DWCU_METHOD_SHB)
+        return pass_x(j, XOP_FWD_SHBP, 1, j->S, j->xa, j->xb, nullptr, shb_alpha(k, j->s.alphamax), 0);
+    return pass_x(j, XOP_FWD_COPY, 1, j->S, j->xa, nullptr, nullptr, 0, 0);
+}
+
+static int alloc_job(dwcu_job *j)
+{
+    const Geometry &g = j->g;
+    const size_t R = sizeof(float) * (size_t) (g.X * g.Y * g.Z);
+    const size_t C = sizeof(float2) * (size_t) (g.XC * g.Y * g.Z);
+    const size_t G = sizeof(float) * (size_t) (g.GP * g.N * g.P);
+    j->nxb = x_blocks(g);
+    j->n_spart = (int) std::min<long long>(1024, g.N * g.P);
+    const long long npsf = g.pM * g.pN * g.pP;
+    j->n_apart = (int) std::min<long long>(1024, (npsf + 4095) / 4096);
+    const bool need_w = j->s.border_quality > 0;
+    size_t off = 0;
+    auto take = [&](size_t b) { size_t o = off; off += align256(b); return o; };
+    size_t o_g = take(G), o_S = take(C), o_K = take(C), o_xa = take(R), o_xb = take(R);
+    size_t o_W = need_w ? take(R) : 0;
+    size_t o_part = take(sizeof(double) * (size_t) j->nxb);
+    size_t o_sc = take(sizeof(JobScalars));
+    size_t o_err = take(sizeof(float) * (size_t) trace_cap(j->s));
+    size_t o_amax = take(sizeof(long long));
+    size_t o_sp = take(sizeof(StatsPartial) * (size_t) j->n_spart);
+    size_t o_ap = take(sizeof(ArgmaxPartial) * (size_t) j->n_apart);
+    size_t o_psf = take(sizeof(float) * (size_t) npsf);
+    j->bytes = off;
+    cudaError_t e = cudaMalloc(&j->base, off);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        j->base = nullptr;
+        return fail(DWCU_ERROR_OUT_OF_MEMORY, "cudaMalloc of %.3f GB for the job failed: %s", off / 1e9,
+                    cudaGetErrorString(e));
+    }
+    char *b = j->base;
+    j->gimg = (float *) (b + o_g);
+    j->S = (float2 *) (b + o_S);
+    j->K = (float2 *) (b + o_K);
+    j->xa = (float *) (b + o_xa);
+    j->xb = (float *) (b + o_xb);
+    j->W = need_w ? (float *) (b + o_W) : nullptr;
+    j->partial = (double *) (b + o_part);
+    j->sc = (JobScalars *) (b + o_sc);
+    j->err = (float *) (b + o_err);
+    j->amax = (long long *) (b + o_amax);
+    j->spart = (StatsPartial *) (b + o_sp);
+    j->apart = (ArgmaxPartial *) (b + o_ap);
+    j->psf_dev = (float *) (b + o_psf);
+    return DWCU_SUCCESS;
+}
+
+static long long job_bytes_estimate(const Geometry &g, const dwcu_opts &s)
+{
+    const long long R = 4LL * g.X * g.Y * g.Z;
+    const long long C = 8LL * g.XC * g.Y * g.Z;
+    const long long G = 4LL * g.GP * g.N * g.P;
+    return G + 2 * C + (s.border_quality > 0 ? 3 : 2) * R + 8LL * ((g.Y * g.Z) / 2 + 1) +
+           4LL * g.pM * g.pN * g.pP + (1 << 20);
+}
+
+static int check_opts(const dwcu_opts &s)
+{
+    if (s.method != DWCU_METHOD_SHB && s.method != DWCU_METHOD_RL)
+        return fail(DWCU_ERROR_INVALID_VALUE, "method must be SHB (2) or RL (0), got %d", s.method);
+    if (s.iter_type < 0 || s.iter_type > 2) return fail(DWCU_ERROR_INVALID_VALUE, "bad iter_type %d", s.iter_type);
+    if (s.n_iter < 0 || s.maxiter < 0) return fail(DWCU_ERROR_INVALID_VALUE, "negative iteration count");
+    if (s.start_condition == DWCU_START_LP)
+        return fail(DWCU_ERROR_UNSUPPORTED, "start_condition LP (Gaussian low-pass start) is not implemented");
+    if (s.start_condition != DWCU_START_FLAT && s.start_condition != DWCU_START_IDENTITY)
+        return fail(DWCU_ERROR_INVALID_VALUE, "bad start_condition %d", s.start_condition);
+    if (s.metric != DWCU_METRIC_IDIV && s.metric != DWCU_METRIC_MSE)
+        return fail(DWCU_ERROR_INVALID_VALUE, "bad metric %d", s.metric);
+    return DWCU_SUCCESS;
+}
+
+static int job_create(long long M, long long N, long long P, long long pM, long long pN, long long pP,
+                      const dwcu_opts *s, dwcu_job **out)
+{
+    *out = nullptr;
+    if (!s) return fail(DWCU_ERROR_INVALID_VALUE, "opts is NULL");
+    TRY(check_opts(*s));
+    Geometry g;
+    TRY(make_geometry(M, N, P, pM, pN, pP, s->border_quality, g));
+    DeviceCtx *ctx = nullptr;
+    TRY(get_ctx(s->device, &ctx));
+    CU(cudaSetDevice(s->device));
+    dwcu_job *j = new dwcu_job();
+    j->s = *s;
+    j->g = g;
+    j->ctx = ctx;
+    j->stream = ctx->stream;
+    int rc = alloc_job(j);
+    if (rc == DWCU_SUCCESS) rc = get_twiddles(ctx, g.X, &j->tw_x);
+    if (rc == DWCU_SUCCESS) rc = get_twiddles(ctx, g.X / 2, &j->tw_l);
+    if (rc == DWCU_SUCCESS && g.Y > 1) rc = get_twiddles(ctx, g.Y, &j->tw_y);
+    if (rc == DWCU_SUCCESS && g.Z > 1) rc = get_twiddles(ctx, g.Z, &j->tw_z);
+    if (rc == DWCU_SUCCESS && cudaMallocHost(&j->h_err, sizeof(float)) != cudaSuccess)
+        rc = fail(DWCU_ERROR_OUT_OF_MEMORY, "pinned allocation failed");
+    if (rc == DWCU_SUCCESS &&
+        (cudaEventCreate(&j->ev0) != cudaSuccess || cudaEventCreate(&j->ev1) != cudaSuccess ||
+         cudaEventCreate(&j->ev2) != cudaSuccess))
+        rc = fail(DWCU_ERROR_CUDA, "event creation failed");
+    if (rc != DWCU_SUCCESS) {
+        dwcu_job_destroy(j);
+        return rc;
+    }
+    j->trace.assign((size_t) trace_cap(*s), 0.f);
+    *out = j;
+    return DWCU_SUCCESS;
+}
+
+// image (compact) into the job's pitched buffer, PSF into staging; then
+// statistics, OTF, weights and the start estimate (method_shb.c:108-296)
+static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_device)
+{
+    const Geometry &g = j->g;
+    CU(cudaSetDevice(j->s.device));
+    cudaStream_t st = j->stream;
+    CU(cudaEventRecord(j->ev0, st));
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CU(cudaMemcpy2DAsync(j->gimg, sizeof(float) * g.GP, im, sizeof(float) * g.M, sizeof(float) * g.M, g.N * g.P,
+                         kind, st));
+    const long long npsf = g.pM * g.pN * g.pP;
+    CU(cudaMemcpyAsync(j->psf_dev, psf, sizeof(float) * npsf, kind, st));
+    CU(cudaMemsetAsync(j->sc, 0, sizeof(JobScalars), st));
+
+    // background and start value
+    const long long nrows = g.N * g.P;
+    const long long rpb = (nrows + j->n_spart - 1) / j->n_spart;
+    const int nsb = (int) ((nrows + rpb - 1) / rpb);
+    k_stats_partial<<<nsb, kRedThreads, 0, st>>>(j->gimg, g.GP, (int) g.M, nrows, rpb, j->spart);
+    CHECK_LAUNCH();
+    k_stats_final<<<1, kRedThreads, 0, st>>>(j->spart, nsb, j->sc, j->s.bg_auto, j->s.bg,
+                                             (unsigned long long) (g.wM * g.wN * g.wP));
+    CHECK_LAUNCH();
+
+    // OTF: PSF with its first maximum at the origin, scaled by 1/(X*Y*Z)
+    const long long per = (npsf + j->n_apart - 1) / j->n_apart;
+    const int nab = (int) ((npsf + per - 1) / per);
+    k_argmax_partial<<<nab, kRedThreads, 0, st>>>(j->psf_dev, npsf, per, j->apart, &j->sc->flags);
+    CHECK_LAUNCH();
+    k_argmax_final<<<1, 32, 0, st>>>(j->apart, nab, j->amax);
+    CHECK_LAUNCH();
+    const size_t R = sizeof(float) * (size_t) (g.X * g.Y * g.Z);
+    CU(cudaMemsetAsync(j->xb, 0, R, st));
+    const float scale = (float) (1.0 / ((double) g.X * (double) g.Y * (double) g.Z));
+    k_psf_embed<<<(int) std::min<long long>(4096, (npsf + 255) / 256), 256, 0, st>>>(
+        j->psf_dev, (int) g.pM, (int) g.pN, (int) g.pP, j->amax, j->xb, (int) g.X, (int) g.Y, (int) g.Z, scale);
+    CHECK_LAUNCH();
+    TRY(pass_x(j, XOP_FWD_COPY, 1, j->K, j->xb, nullptr, nullptr, 0, 0));
+    TRY(pass_y(j, LINES_FWD, j->K));
+    TRY(pass_z(j, LINES_FWD, j->K));
+
+    // Bertero weights: W = 1/P1 where P1 = K^T 1_image > 0.01 (method_shb.c:216-235)
+    if (j->W) {
+        TRY(pass_x(j, XOP_FWD_ONES, 1, j->S, nullptr, nullptr, nullptr, 0, 0));
+        TRY(conv(j, 1));
+        TRY(pass_x(j, XOP_WEIGHTS, 0, j->S, nullptr, nullptr, j->W, 0, 0));
+    }
+
+    // start estimate (method_shb.c:264-276); x_{-1} = x_0
+    const long long nv = g.X * g.Y * g.Z;
+    const int fb = (int) std::min<long long>(148 * 16, (nv + 255) / 256);
+    if (j->s.start_condition == DWCU_START_FLAT) {
+        k_fill_scalar<<<fb, 256, 0, st>>>(j->xa, nv, j->sc);
+        CHECK_LAUNCH();
+    } else {
+        CU(cudaMemsetAsync(j->xa, 0, R, st));
+        k_embed_image<<<fb, 256, 0, st>>>(j->gimg, g.GP, (int) g.M, (int) g.N, (int) g.P, j->xa, (int) g.X,
+                                          (int) g.Y);
+        CHECK_LAUNCH();
+    }
+    if (j->s.method == DWCU_METHOD_SHB) CU(cudaMemcpyAsync(j->xb, j->xa, R, cudaMemcpyDeviceToDevice, st));
+
+    // input flags (non-finite values) are checked once, here
+    JobScalars hs;
+    CU(cudaMemcpyAsync(&hs, j->sc, sizeof hs, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (hs.flags & 1) return fail(DWCU_ERROR_INPUT, "the image contains non-finite values");
+    if (hs.flags & 2) return fail(DWCU_ERROR_INPUT, "the PSF contains non-finite values");
+    if (j->s.bg_auto) j->s.bg = hs.bg;
+    j->it.init(j->s);
+    j->k_next = j->it.next();
+    j->finished = (j->k_next < 0);
+    j->spectrum_ready = false;
+    j->done_iters = 0;
+    j->setup_done = true;
+    CU(cudaEventRecord(j->ev1, st));
+    return DWCU_SUCCESS;
+}
+
+// Enqueue iterations.  FIXED: no host synchronisation (and, if requested, the
+// whole remaining loop as one CUDA graph).  REL/ABS: each error is read back
+// before deciding whether the next iteration runs (dw.c:237-270).
+static int job_step(dwcu_job *j, int nmax, int *remaining)
+{
+    if (!j->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "job_step before job_setup");
+    CU(cudaSetDevice(j->s.device));
+    const bool shb = (j->s.method == DWCU_METHOD_SHB);
+    const bool fixed = (j->s.iter_type == DWCU_ITER_FIXED);
+    int ran = 0;
+    auto run_one_fixed = [&](int k) -> int {
+        const bool last = (k == j->it.niter - 1);
+        if (!j->spectrum_ready) TRY(iter_input(j, k));
+        // SHB's last update is discarded (method_shb.c:385-395): only its error is needed
+        TRY(iter_forward(j, k, !(last && shb)));
+        if (!(last && shb)) TRY(iter_backward(j, k, !last));
+        j->spectrum_ready = !last;
+        return DWCU_SUCCESS;
+    };
+    while (!j->finished && ran < nmax) {
+        const int k = j->k_next;
+        if (fixed) {
+            const bool use_graph = j->s.use_graph && nmax >= (j->it.niter - k) && (j->it.niter - k) > 1 && !j->graph;
+            if (use_graph) {
+                // capture the whole remaining loop into one graph
+                cudaGraph_t gr = nullptr;
+                CU(cudaStreamBeginCapture(j->stream, cudaStreamCaptureModeThreadLocal));
+                int rc = DWCU_SUCCESS;
+                for (int kk = k; kk < j->it.niter && rc == DWCU_SUCCESS; ++kk) rc = run_one_fixed(kk);
+                cudaError_t ce = cudaStreamEndCapture(j->stream, &gr);
+                if (rc != DWCU_SUCCESS) {
+                    if (gr) cudaGraphDestroy(gr);
+                    return rc;
+                }
+                if (ce != cudaSuccess) return fail(DWCU_ERROR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+                cudaGraphExec_t ex = nullptr;
+                ce = cudaGraphInstantiate(&ex, gr, 0);
+                cudaGraphDestroy(gr);
+                if (ce != cudaSuccess) return fail(DWCU_ERROR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+                CU(cudaGraphLaunch(ex, j->stream));  // its kernels were counted at capture
+                j->graph = ex;
+                ran += j->it.niter - k;
+                j->done_iters = j->it.niter;
+                j->it.iter = j->it.niter;
+                j->k_next = -1;
+                j->finished = true;
+                break;
+            }
+            TRY(run_one_fixed(k));
+            ran++;
+            j->done_iters = k + 1;
+            j->k_next = (k + 1 < j->it.niter) ? k + 1 : -1;
+            j->it.iter = k;
+            if (j->k_next < 0) j->finished = true;
+            continue;
+        }
+        // REL / ABS: forward half, read the error, decide
+        if (!j->spectrum_ready) TRY(iter_input(j, k));
+        TRY(iter_forward(j, k, true));
+        CU(cudaMemcpyAsync(j->h_err, j->err + k, sizeof(float), cudaMemcpyDeviceToHost, j->stream));
+        CU(cudaStreamSynchronize(j->stream));
+        const float e = *j->h_err;
+        j->it.set(e);
+        j->trace[(size_t) k] = e;
+        j->done_iters = k + 1;
+        if (j->s.verbosity > 0) printf("Iteration %3d/%3d, %s=%.3e\n", k + 1, j->it.niter,
+                                       j->s.metric == DWCU_METRIC_IDIV ? "Idiv" : "fMSE", e);
+        const int kn = j->it.next();
+        ran++;
+        if (kn >= 0) {
+            TRY(iter_backward(j, k, true));
+            j->spectrum_ready = true;
+            j->k_next = kn;
+        } else {
+            if (!shb) TRY(iter_backward(j, k, false));  // RL returns x_{k+1}
+            j->spectrum_ready = false;
+            j->k_next = -1;
+            j->finished = true;
+        }
+    }
+    if (remaining) {
+        if (j->finished) *remaining = 0;
+        else *remaining = fixed ? (j->it.niter - j->k_next) : (j->it.niter - j->k_next);
+    }
+    return DWCU_SUCCESS;
+}
+
+// result: SHB's output is x_{N-1}, i.e. the estimate the last forward half
+// read; RL's is x_N.  Both live in xa when the loop has finished.
+static int job_result(dwcu_job *j, float *out, bool on_device, dwcu_opts *so)
+{
+    const Geometry &g = j->g;
+    CU(cudaSetDevice(j->s.device));
+    if (!j->finished) return fail(DWCU_ERROR_NOT_READY, "the job has iterations left");
+    cudaStream_t st = j->stream;
+    float *dout = out;
+    float *tmp = nullptr;
+    if (!on_device) {
+        // crop on the device into the S buffer (free now), then one copy
+        tmp = reinterpret_cast<float *>(j->S);
+        dout = tmp;
+    }
+    const long long n = g.M * g.N * g.P;
+    const int fb = (int) std::min<long long>(148 * 16, (n + 255) / 256);
+    k_crop<<<fb, 256, 0, st>>>(j->xa, (int) g.X, (int) g.Y, (int) g.M, (int) g.N, (int) g.P, dout);
+    CHECK_LAUNCH();
+    CU(cudaEventRecord(j->ev2, st));
+    if (!on_device) CU(cudaMemcpyAsync(out, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    const int nerr = j->done_iters;
+    std::vector<float> errs((size_t) std::max(1, nerr));
+    if (nerr > 0) CU(cudaMemcpyAsync(errs.data(), j->err, sizeof(float) * nerr, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (so) {
+        so->iterations_done = nerr;
+        so->bg = j->s.bg;
+        so->work[0] = g.X; so->work[1] = g.Y; so->work[2] = g.Z;
+        float ms_setup = 0, ms_loop = 0;
+        cudaEventElapsedTime(&ms_setup, j->ev0, j->ev1);
+        cudaEventElapsedTime(&ms_loop, j->ev1, j->ev2);
+        so->seconds_setup = ms_setup * 1e-3;
+        so->seconds_iterate = ms_loop * 1e-3;
+        if (so->error_trace)
+            for (int i = 0; i < nerr && i < so->trace_capacity; ++i) so->error_trace[i] = errs[(size_t) i];
+        if (j->s.verbosity > 0 && j->s.iter_type == DWCU_ITER_FIXED)
+            for (int i = 0; i < nerr; ++i)
+                printf("Iteration %3d/%3d, %s=%.3e\n", i + 1, nerr,
+                       j->s.metric == DWCU_METRIC_IDIV ? "Idiv" : "fMSE", errs[(size_t) i]);
+    }
+    return DWCU_SUCCESS;
+}
+
+static int one_call(const float *im, long long M, long long N, long long P, const float *psf, long long pM,
+                    long long pN, long long pP, dwcu_opts *s, float *out, bool on_device, cudaStream_t stream)
+{
+    if (!s || !im || !psf || !out) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    s->iterations_done = 0;
+    if (s->n_iter == 0) {
+        // method_shb.c:101-105: nIter == 0 returns a copy of the image
+        if (on_device) {
+            CU(cudaSetDevice(s->device));
+            CU(cudaMemcpyAsync(out, im, sizeof(float) * M * N * P, cudaMemcpyDeviceToDevice, stream));
+            CU(cudaStreamSynchronize(stream));
+        } else {
+            memcpy(out, im, sizeof(float) * (size_t) (M * N * P));
+        }
+        return DWCU_SUCCESS;
+    }
+    dwcu_job *j = nullptr;
+    TRY(job_create(M, N, P, pM, pN, pP, s, &j));
+    if (on_device && stream) j->stream = stream;
+    int rc = job_setup(j, im, psf, on_device);
+    if (rc == DWCU_SUCCESS) rc = job_step(j, 1 << 30, nullptr);
+    if (rc == DWCU_SUCCESS) rc = job_result(j, out, on_device, s);
+    if (rc == DWCU_SUCCESS && s->bg_auto) s->bg = j->s.bg;
+    dwcu_job_destroy(j);
+    return rc;
+}
+
+// standalone 3-D transforms on exact sizes (fft.c's fft()/ifft())
+static int fft3d(const float *d_in, long long M, long long N, long long P, float *d_out, int device,
+                 cudaStream_t stream, bool forward)
+{
+    if (!d_in || !d_out) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    if (M < 2 || N < 1 || P < 1 || (M % 2)) return fail(DWCU_ERROR_INVALID_VALUE, "M must be even and >= 2");
+    DeviceCtx *ctx = nullptr;
+    TRY(get_ctx(device, &ctx));
+    CU(cudaSetDevice(device));
+    dwcu_job jj;
+    dwcu_job *j = &jj;
+    Geometry &g = j->g;
+    g.M = M; g.N = N; g.P = P; g.pM = g.pN = g.pP = 1;
+    g.wM = g.X = M; g.wN = g.Y = N; g.wP = g.Z = P;
+    g.xp = find_x((int) (M / 2));
+    g.yp = N > 1 ? find_lines((int) N) : nullptr;
+    g.zp = P > 1 ? find_lines((int) P) : nullptr;
+    if (!g.xp || (N > 1 && !g.yp) || (P > 1 && !g.zp))
+        return fail(DWCU_ERROR_UNSUPPORTED, "unsupported transform size %lld x %lld x %lld", M, N, P);
+    g.XC = (M / 2 + 1 + 1) & ~1LL;
+    g.GP = (M + 1) & ~1LL;
+    j->s.metric = DWCU_METRIC_IDIV;
+    j->s.positivity = 1;
+    j->ctx = ctx;
+    j->stream = stream ? stream : ctx->stream;
+    j->nxb = x_blocks(g);
+    TRY(get_twiddles(ctx, g.X, &j->tw_x));
+    TRY(get_twiddles(ctx, g.X / 2, &j->tw_l));
+    if (N > 1) TRY(get_twiddles(ctx, N, &j->tw_y));
+    if (P > 1) TRY(get_twiddles(ctx, P, &j->tw_z));
+    const size_t C = sizeof(float2) * (size_t) (g.XC * N * P);
+    void *tmp = nullptr;
+    CU(cudaMalloc(&tmp, C + sizeof(JobScalars) + 256));
+    j->S = (float2 *) tmp;
+    j->sc = (JobScalars *) ((char *) tmp + align256(C));
+    j->K = nullptr;
+    j->W = nullptr;
+    j->partial = nullptr;
+    int rc = DWCU_SUCCESS;
+    const size_t hw = sizeof(float2) * (size_t) (M / 2 + 1);
+    if (cudaMemsetAsync(j->sc, 0, sizeof(JobScalars), j->stream) != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "memset");
+    if (forward) {
+        if (rc == DWCU_SUCCESS) rc = pass_x(j, XOP_FWD_COPY, 1, j->S, d_in, nullptr, nullptr, 0, 0);
+        if (rc == DWCU_SUCCESS) rc = pass_y(j, LINES_FWD, j->S);
+        if (rc == DWCU_SUCCESS) rc = pass_z(j, LINES_FWD, j->S);
+        if (rc == DWCU_SUCCESS && cudaMemcpy2DAsync(d_out, hw, j->S, sizeof(float2) * g.XC, hw, N * P,
+                                                    cudaMemcpyDeviceToDevice, j->stream) != cudaSuccess)
+            rc = fail(DWCU_ERROR_CUDA, "copy failed");
+    } else {
+        if (cudaMemcpy2DAsync(j->S, sizeof(float2) * g.XC, d_in, hw, hw, N * P, cudaMemcpyDeviceToDevice,
+                              j->stream) != cudaSuccess)
+            rc = fail(DWCU_ERROR_CUDA, "copy failed");
+        if (rc == DWCU_SUCCESS) rc = pass_z(j, LINES_INV, j->S);
+        if (rc == DWCU_SUCCESS) rc = pass_y(j, LINES_INV, j->S);
+        if (rc == DWCU_SUCCESS) rc = pass_x(j, XOP_STORE, 0, j->S, nullptr, nullptr, d_out, 0, 0);
+    }
+    cudaError_t e = cudaStreamSynchronize(j->stream);
+    cudaFree(tmp);
+    j->base = nullptr;
+    j->ev0 = j->ev1 = j->ev2 = nullptr;
+    j->stream = nullptr;
+    if (rc != DWCU_SUCCESS) return rc;
+    if (e != cudaSuccess) return fail(DWCU_ERROR_CUDA, "transform failed: %s", cudaGetErrorString(e));
+    return DWCU_SUCCESS;
+}
+
+}  // namespace dwcu
+
+// ================================================================ C ABI
+
+using namespace dwcu;
+
+extern "C" {
+
+void dwcu_opts_init(dwcu_opts *s)
+{
+    if (!s) return;
+    memset(s, 0, sizeof *s);
+    s->method = DWCU_METHOD_SHB;
+    s->n_iter = 1;
+    s->iter_type = DWCU_ITER_REL;
+    s->maxiter = 250;
+    s->err_rel = 0.02f;
+    s->err_abs = 1.0f;
+    s->bg = 1e-2f;
+    s->bg_auto = 1;
+    s->positivity = 1;
+    s->border_quality = 2;
+    s->start_condition = DWCU_START_FLAT;
+    s->metric = DWCU_METRIC_IDIV;
+    s->alphamax = 1.0f;
+    s->device = 0;
+    s->verbosity = 0;
+    s->use_graph = 1;
+}
+
+int dwcu_deconvolve(const float *im, int64_t M, int64_t N, int64_t P, const float *psf, int64_t pM, int64_t pN,
+                    int64_t pP, dwcu_opts *s, float *out)
+{
+    return one_call(im, M, N, P, psf, pM, pN, pP, s, out, false, nullptr);
+}
+
+int dwcu_deconvolve_device(const float *d_im, int64_t M, int64_t N, int64_t P, const float *d_psf, int64_t pM,
+                           int64_t pN, int64_t pP, dwcu_opts *s, float *d_out, void *stream)
+{
+    return one_call(d_im, M, N, P, d_psf, pM, pN, pP, s, d_out, true, (cudaStream_t) stream);
+}
+
+int dwcu_plan_size(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP, int32_t border_quality,
+                   int32_t method, int64_t work[3], int64_t *device_bytes)
+{
+    Geometry g;
+    int rc = make_geometry(M, N, P, pM, pN, pP, border_quality, g);
+    if (rc != DWCU_SUCCESS) return rc;
+    if (work) { work[0] = g.X; work[1] = g.Y; work[2] = g.Z; }
+    dwcu_opts s;
+    dwcu_opts_init(&s);
+    s.border_quality = border_quality;
+    s.method = method;
+    if (device_bytes) *device_bytes = job_bytes_estimate(g, s);
+    return DWCU_SUCCESS;
+}
+
+int dwcu_job_create(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP, const dwcu_opts *s,
+                    dwcu_job **job)
+{
+    if (!job) return fail(DWCU_ERROR_INVALID_VALUE, "job is NULL");
+    return job_create(M, N, P, pM, pN, pP, s, job);
+}
+
+int dwcu_job_setup(dwcu_job *job, const float *im, const float *psf, int32_t on_device)
+{
+    if (!job || !im || !psf) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    return job_setup(job, im, psf, on_device != 0);
+}
+
+int dwcu_job_step(dwcu_job *job, int32_t n, int32_t *remaining)
+{
+    if (!job) return fail(DWCU_ERROR_INVALID_VALUE, "job is NULL");
+    return job_step(job, n, remaining);
+}
+
+int dwcu_job_done(const dwcu_job *job) { return job && job->finished ? 1 : 0; }
+
+int dwcu_job_result(dwcu_job *job, float *out, int32_t out_on_device, dwcu_opts *s_out)
+{
+    if (!job || !out) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    return job_result(job, out, out_on_device != 0, s_out);
+}
+
+void dwcu_job_destroy(dwcu_job *j)
+{
+    if (!j) return;
+    cudaSetDevice(j->s.device);
+    if (j->stream) cudaStreamSynchronize(j->stream);
+    if (j->graph) cudaGraphExecDestroy(j->graph);
+    if (j->base) cudaFree(j->base);
+    if (j->h_err) cudaFreeHost(j->h_err);
+    if (j->ev0) cudaEventDestroy(j->ev0);
+    if (j->ev1) cudaEventDestroy(j->ev1);
+    if (j->ev2) cudaEventDestroy(j->ev2);
+    delete j;
+}
+
+int dwcu_job_set_stream(dwcu_job *job, void *stream)
+{
+    if (!job) return fail(DWCU_ERROR_INVALID_VALUE, "job is NULL");
+    job->stream = stream ? (cudaStream_t) stream : job->ctx->stream;
+    return DWCU_SUCCESS;
+}
+
+int64_t dwcu_job_bytes(const dwcu_job *job) { return job ? (int64_t) job->bytes : 0; }
+
+const char *dwcu_last_error(void) { return g_last_error.c_str(); }
+int dwcu_abi_version(void) { return DWCU_ABI_VERSION; }
+int dwcu_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+int64_t dwcu_launch_count(void) { return g_launches; }
+
+int dwcu_profile_enable(int32_t on)
+{
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof_on = on != 0;
+    return DWCU_SUCCESS;
+}
+
+int dwcu_profile_collect(dwcu_kernel_stat *stats, int32_t capacity, int32_t *count)
+{
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    std::vector<double> ms(g_prof_classes.size(), 0.0);
+    std::vector<long long> n(g_prof_classes.size(), 0);
+    for (auto &r : g_prof_recs) {
+        if (cudaEventSynchronize(r.b) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+            ms[(size_t) r.cls] += t;
+            n[(size_t) r.cls] += 1;
+        } else {
+            cudaGetLastError();
+        }
+        g_prof_pool.push_back(r.a);
+        g_prof_pool.push_back(r.b);
+    }
+    g_prof_recs.clear();
+    int k = 0;
+    for (size_t i = 0; i < g_prof_classes.size(); ++i) {
+        if (n[i] == 0) continue;
+        if (stats && k < capacity) {
+            memset(&stats[k], 0, sizeof stats[k]);
+            snprintf(stats[k].name, sizeof stats[k].name, "%s", g_prof_classes[i].name.c_str());
+            stats[k].launches = n[i];
+            stats[k].milliseconds = ms[i];
+            stats[k].bytes_per_launch = g_prof_classes[i].bytes;
+        }
+        ++k;
+    }
+    if (count) *count = k;
+    return DWCU_SUCCESS;
+}
+
+int dwcu_fft_r2c(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_out, int32_t device, void *stream)
+{
+    return fft3d(d_in, M, N, P, d_out, device, (cudaStream_t) stream, true);
+}
+
+int dwcu_fft_c2r(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_out, int32_t device, void *stream)
+{
+    return fft3d(d_in, M, N, P, d_out, device, (cudaStream_t) stream, false);
+}
+
+}  // extern "C"

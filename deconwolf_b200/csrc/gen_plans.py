@@ -1,0 +1,187 @@
+"""Generate the per-length kernel instantiations of the FFT passes.
+
+Writes, next to this file:
+  plans_gen.h         the table of supported line lengths with their radix
+                      lists and launch shapes (lines: T lines per CTA;
+                      x pass: R rows per CTA)
+  inst_lines_<k>.cu   explicit instantiations of k_lines, split for parallel
+  inst_x_<k>.cu       and k_xpass, compilation
+
+A length N is supported when it factors into at most three radices <= 16
+(7-smooth).  The radix list is chosen to minimise the threads per line
+(N / smallest radix), then the number of stages, then the spread.
+Run: python gen_plans.py [--max 4096] [--parts 8]
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def factors(n):
+    out = []
+    for p in (2, 3, 5, 7):
+        while n % p == 0:
+            out.append(p)
+            n //= p
+    return out, n
+
+
+def smooth(n):
+    return factors(n)[1] == 1
+
+
+RADS = [r for r in range(2, 17) if smooth(r)]
+
+
+def tpl_of(n, s):
+    return max(n // s[0], n // s[1], n // s[2] if s[2] > 1 else 0)
+
+
+def best_split(n):
+    """(RA, RB, RC) with RA*RB*RC == n, radices in RADS (RB, RC may be 1)."""
+    if n == 1:
+        return None
+    cands = []
+    if n in RADS:
+        cands.append((n, 1, 1))
+    for a in RADS:
+        if n % a:
+            continue
+        b = n // a
+        if b in RADS:
+            cands.append((a, b, 1))
+        for c in RADS:
+            if b % c == 0 and (b // c) in RADS:
+                cands.append((a, c, b // c))
+    if not cands:
+        return None
+
+    def key(s):
+        rs = [r for r in s if r > 1]
+        stages = 3 if s[2] > 1 else 2
+        if len(rs) == 1:
+            stages = 1
+        tpl = tpl_of(n, s)
+        # prefer a large first radix (it reads global memory with the most
+        # independent loads per thread) and a moderate last one
+        return (tpl, stages, max(rs) - min(rs), -s[0])
+
+    return min(cands, key=key)
+
+
+def lines_T(n, split):
+    """Lines per CTA for the strided passes: as many as fit 1024 threads and
+    ~100 KB of shared memory, at most 16 (128-byte segments)."""
+    a, b, c = split
+    rev = (c, b, a) if c > 1 else (b, a, 1)
+    tpl = max(tpl_of(n, split), tpl_of(n, rev))
+    padn = n + n // min(a, rev[0]) + 1
+    T = 16
+    while T > 1 and (T * tpl > 1024 or T * padn * 8 > 100 * 1024):
+        T //= 2
+    return T, tpl
+
+
+def x_R(n, split):
+    """Rows per CTA for the x pass (complex half length n)."""
+    a, b, c = split
+    rev = (c, b, a) if c > 1 else (b, a, 1)
+    tpl = max(tpl_of(n, split), tpl_of(n, rev))
+    row = (max(n + 1, n + n // min(a, rev[0]) + 1)) | 1
+    R = 1
+    while (2 * R) * tpl <= 512 and (2 * R) * row * 8 <= 48 * 1024 and R < 8:
+        R *= 2
+    while R * tpl < 32:
+        R *= 2
+    return R, tpl
+
+
+def supported(maxn):
+    out = []
+    for n in range(2, maxn + 1):
+        if smooth(n) and best_split(n):
+            out.append(n)
+    return out
+
+
+def rad_str(s):
+    return f"Rad<{s[0]}, {s[1]}, {s[2]}>"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--max", type=int, default=4096)
+    ap.add_argument("--xmax", type=int, default=2048, help="largest complex half length of the x pass")
+    ap.add_argument("--parts", type=int, default=8)
+    ap.add_argument("--only", type=str, default="", help="comma list of lengths (development builds)")
+    args = ap.parse_args()
+
+    lines_ns = supported(args.max)
+    x_ns = supported(args.xmax)
+    if args.only:
+        keep = {int(v) for v in args.only.split(",")}
+        lines_ns = [n for n in lines_ns if n in keep]
+        x_ns = [n for n in x_ns if n in keep]
+
+    hdr = []
+    hdr.append("// generated by gen_plans.py -- do not edit")
+    hdr.append("#pragma once")
+    hdr.append("#include \"passes.cuh\"")
+    hdr.append("namespace dwcu {")
+    hdr.append("struct LinesPlan { int n, ra, rb, rc, T, threads; size_t smem; void (*launch)(const LinesArgs &, int, cudaStream_t); };")
+    hdr.append("struct XPlan { int n, ra, rb, rc, R, threads; size_t smem; void (*launch)(const XArgs &, int, cudaStream_t); };")
+    for n in lines_ns:
+        s = best_split(n)
+        T, _ = lines_T(n, s)
+        hdr.append(f"void launch_lines_{n}(const LinesArgs &, int, cudaStream_t);")
+    for n in x_ns:
+        hdr.append(f"void launch_x_{n}(const XArgs &, int, cudaStream_t);")
+    hdr.append("static const LinesPlan kLinesPlans[] = {")
+    for n in lines_ns:
+        s = best_split(n)
+        T, _ = lines_T(n, s)
+        hdr.append(f"    {{{n}, {s[0]}, {s[1]}, {s[2]}, {T}, LinesCfg<{rad_str(s)}, {T}>::THREADS, "
+                   f"LinesCfg<{rad_str(s)}, {T}>::SMEM_BYTES, launch_lines_{n}}},")
+    hdr.append("};")
+    hdr.append("static const XPlan kXPlans[] = {")
+    for n in x_ns:
+        s = best_split(n)
+        R, _ = x_R(n, s)
+        hdr.append(f"    {{{n}, {s[0]}, {s[1]}, {s[2]}, {R}, XCfg<{rad_str(s)}, {R}>::THREADS, "
+                   f"XCfg<{rad_str(s)}, {R}>::SMEM_BYTES, launch_x_{n}}},")
+    hdr.append("};")
+    hdr.append("}  // namespace dwcu")
+    with open(os.path.join(HERE, "plans_gen.h"), "w") as f:
+        f.write("\n".join(hdr) + "\n")
+
+    # instantiation files
+    for old in os.listdir(HERE):
+        if old.startswith("inst_") and old.endswith(".cu"):
+            os.remove(os.path.join(HERE, old))
+    parts = max(1, args.parts)
+    for kind, ns in (("lines", lines_ns), ("x", x_ns)):
+        for p in range(parts):
+            chunk = ns[p::parts]
+            lines = ["// generated by gen_plans.py -- do not edit", "#include \"launch.cuh\"", "namespace dwcu {"]
+            for n in chunk:
+                s = best_split(n)
+                if kind == "lines":
+                    T, _ = lines_T(n, s)
+                    lines.append(f"void launch_lines_{n}(const LinesArgs &a, int nb, cudaStream_t st) "
+                                 f"{{ launch_lines_t<{rad_str(s)}, {T}>(a, nb, st); }}")
+                else:
+                    R, _ = x_R(n, s)
+                    lines.append(f"void launch_x_{n}(const XArgs &a, int nb, cudaStream_t st) "
+                                 f"{{ launch_x_t<{rad_str(s)}, {R}>(a, nb, st); }}")
+            lines.append("}  // namespace dwcu")
+            with open(os.path.join(HERE, f"inst_{kind}_{p}.cu"), "w") as f:
+                f.write("\n".join(lines) + "\n")
+    print(f"lines lengths: {len(lines_ns)}  x half-lengths: {len(x_ns)}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,189 @@
+/* dwcu.h -- C ABI of the B200-native Richardson-Lucy / Scaled-Heavy-Ball engine.
+ *
+ * This is the drop-in boundary for deconwolf's `dw --method shb|rl --gpu` path.
+ * deconwolf selects its deconvolution method through a function pointer,
+ *
+ *     typedef float * (*dw_function)(float * restrict im, int64_t M, N, P,
+ *                                    float * restrict psf, int64_t pM, pN, pP,
+ *                                    dw_opts * s);                (src/dw.h:89-91)
+ *
+ * called from dw_run (src/dw.c:2841) and deconvolve_tiles (src/dw.c:2137).
+ * dwcu_deconvolve() below is that call with plain C types: the dw_opts fields
+ * the iteration honours are carried in dwcu_opts, the result goes to a caller
+ * buffer, and failures return a status instead of exit().  The reference-side
+ * glue that adapts dw_opts and registers deconvolve_shb_cu / deconvolve_rl_cu
+ * as dw_functions is shown in INTEGRATION.md.
+ *
+ * Layout everywhere: float32, x fastest, index = m + n*M + p*M*N (deconwolf's
+ * fim layout), no row padding at this boundary.
+ *
+ * All functions return 0 (DWCU_SUCCESS) or a positive dwcu_status; the text
+ * of the last failure on the calling thread is dwcu_last_error().  No
+ * function falls back to the CPU: without a usable CUDA device every compute
+ * call fails with DWCU_ERROR_CUDA.
+ */
+#ifndef DWCU_H
+#define DWCU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DWCU_ABI_VERSION 1
+
+typedef enum dwcu_status {
+    DWCU_SUCCESS = 0,
+    DWCU_ERROR_INVALID_VALUE = 1, /* bad argument (sizes, null pointers, options) */
+    DWCU_ERROR_UNSUPPORTED = 2,   /* valid for deconwolf, not implemented here (e.g. --start_lp) */
+    DWCU_ERROR_OUT_OF_MEMORY = 3, /* device allocation failed or HBM budget exceeded */
+    DWCU_ERROR_CUDA = 4,          /* CUDA runtime / launch failure, or no device */
+    DWCU_ERROR_INPUT = 5,         /* non-finite image or PSF values */
+    DWCU_ERROR_NOT_READY = 6,     /* asynchronous work still running */
+    DWCU_ERROR_CANCELLED = 7,     /* a job was cancelled before it finished */
+    DWCU_ERROR_TIMEOUT = 8,       /* a bounded wait gave up */
+    DWCU_ERROR_INTERNAL = 9
+} dwcu_status;
+
+/* Enum values equal deconwolf's own (src/dw.h:52-83). */
+enum { DWCU_METHOD_RL = 0, DWCU_METHOD_SHB = 2 };
+enum { DWCU_START_FLAT = 0, DWCU_START_LP = 1, DWCU_START_IDENTITY = 2 };
+enum { DWCU_METRIC_MSE = 0, DWCU_METRIC_IDIV = 1 };
+enum { DWCU_ITER_ABS = 0, DWCU_ITER_REL = 1, DWCU_ITER_FIXED = 2 };
+
+/* The dw_opts fields the iteration reads (src/dw.h:104-211), same meaning. */
+typedef struct dwcu_opts {
+    int32_t method;          /* DWCU_METHOD_SHB (default) or DWCU_METHOD_RL   (dw_opts.method) */
+    int32_t n_iter;          /* iterations for DWCU_ITER_FIXED               (dw_opts.nIter) */
+    int32_t iter_type;       /* stopping rule, default DWCU_ITER_REL          (dw_opts.iter_type) */
+    int32_t maxiter;         /* cap for REL / ABS, default 250                (dw_opts.maxiter) */
+    float err_rel;           /* REL threshold, default 0.02                   (dw_opts.err_rel) */
+    float err_abs;           /* ABS threshold                                  (dw_opts.err_abs) */
+    float bg;                /* background; overwritten when bg_auto          (dw_opts.bg) */
+    int32_t bg_auto;         /* 1: bg = max(min(image), 0.01), default 1       (dw_opts.bg_auto) */
+    int32_t positivity;      /* SHB: clamp the estimate at bg, default 1      (dw_opts.positivity) */
+    int32_t border_quality;  /* 2 (default); 1 and 0 need exact-size FFTs    (dw_opts.borderQuality) */
+    int32_t start_condition; /* FLAT (default) or IDENTITY                    (dw_opts.start_condition) */
+    int32_t metric;          /* IDIV (default) or MSE                         (dw_opts.metric) */
+    float alphamax;          /* SHB extrapolation cap, default 1              (dw_opts.alphamax) */
+    int32_t device;          /* CUDA device ordinal                            (dw_opts.cl_device) */
+    int32_t verbosity;       /* 0 silent; > 0 prints per-iteration lines      (dw_opts.verbosity) */
+    int32_t use_graph;       /* FIXED iterations: capture the loop in a CUDA graph (default 1) */
+    /* outputs */
+    int32_t iterations_done; /* iterations run */
+    float *error_trace;      /* optional host array: error of each iteration */
+    int32_t trace_capacity;  /* its length */
+    int64_t work[3];         /* padded job size used (X, Y, Z) */
+    double seconds_setup;    /* device time before the first iteration */
+    double seconds_iterate;  /* device time of the iteration loop */
+} dwcu_opts;
+
+/* Defaults of dw_opts_new (src/dw.c:340-413) for the fields above. */
+void dwcu_opts_init(dwcu_opts *s);
+
+/* ---------------------------------------------------------------- one call */
+
+/* Deconvolve the host image im (M x N x P) with the host PSF (pM x pN x pP)
+ * into the host buffer out (M x N x P).  Replaces the dw_function call
+ * s->fun(im, M, N, P, psf, pM, pN, pP, s) (src/dw.c:2841) for the methods
+ * deconvolve_shb (src/method_shb.c:77-424), deconvolve_rl
+ * (src/method_rl.c:105-400) and deconvolve_shb_cl2 (src/method_shb_cl2.c:
+ * 166-602).  im and psf are only read.  SHB returns the iterate before the
+ * last update (method_shb.c:385-395), RL the last one (method_rl.c:393);
+ * n_iter == 0 copies the image (method_shb.c:101-105). */
+int dwcu_deconvolve(const float *im, int64_t M, int64_t N, int64_t P,
+                    const float *psf, int64_t pM, int64_t pN, int64_t pP,
+                    dwcu_opts *s, float *out);
+
+/* Same with device-resident buffers (device s->device): d_im, d_psf and d_out
+ * are device pointers; work is ordered on `stream` (a cudaStream_t, NULL for
+ * the default stream) and the call returns after it completes. */
+int dwcu_deconvolve_device(const float *d_im, int64_t M, int64_t N, int64_t P,
+                           const float *d_psf, int64_t pM, int64_t pN, int64_t pP,
+                           dwcu_opts *s, float *d_out, void *stream);
+
+/* The padded job size (X, Y, Z) the engine uses for these sizes, and the
+ * device bytes one job needs.  Returns DWCU_ERROR_UNSUPPORTED when no
+ * supported FFT length covers the job (see border_quality). */
+int dwcu_plan_size(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP,
+                   int32_t border_quality, int32_t method, int64_t work[3], int64_t *device_bytes);
+
+/* ---------------------------------------------------------------- jobs */
+
+/* A job keeps its image, OTF, weights and estimates resident on the device
+ * so that many jobs (tiles, channels, requests) can be stepped in any
+ * interleaving.  Jobs created on the same device share that device's stream
+ * unless dwcu_job_set_stream is called. */
+typedef struct dwcu_job dwcu_job;
+
+/* Allocate a job for an M x N x P image and pM x pN x pP PSF with options s
+ * (copied).  Returns DWCU_ERROR_OUT_OF_MEMORY when the device allocation
+ * fails. */
+int dwcu_job_create(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP,
+                    const dwcu_opts *s, dwcu_job **job);
+/* Upload image and PSF (host pointers, or device pointers when on_device)
+ * and run the setup: background, OTF, Bertero weights, start estimate. */
+int dwcu_job_setup(dwcu_job *job, const float *im, const float *psf, int32_t on_device);
+/* Enqueue up to n more iterations (without waiting).  The stopping rule of
+ * s->iter_type is applied; REL and ABS read each error back (one small copy
+ * per iteration).  *remaining receives how many iterations may still run. */
+int dwcu_job_step(dwcu_job *job, int32_t n, int32_t *remaining);
+/* 1 when the job has finished all its iterations. */
+int dwcu_job_done(const dwcu_job *job);
+/* Wait for the job's queued work; copy the result (host or device pointer)
+ * and the error trace.  Fills s-like outputs into *s_out when non-NULL. */
+int dwcu_job_result(dwcu_job *job, float *out, int32_t out_on_device, dwcu_opts *s_out);
+/* Release all device memory of the job. */
+void dwcu_job_destroy(dwcu_job *job);
+/* Use a caller stream (cudaStream_t) for this job's work. */
+int dwcu_job_set_stream(dwcu_job *job, void *stream);
+/* Device bytes held by the job. */
+int64_t dwcu_job_bytes(const dwcu_job *job);
+
+/* ---------------------------------------------------------------- FFT */
+
+/* 3-D real-to-complex transform of d_in (M x N x P floats, device) into
+ * d_out ((M/2+1) x N x P interleaved complex, device), unnormalised, the
+ * layout of fftwf_plan_dft_r2c_3d(P, N, M, ...).  Replaces fft() (src/fft.c:
+ * 401-415).  M must be even with M/2, N and P supported lengths. */
+int dwcu_fft_r2c(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_out, int32_t device,
+                 void *stream);
+/* Complex-to-real inverse of the above, unnormalised (the caller divides by
+ * M*N*P as ifft() does, src/fft.c:383-398).  d_in is not modified. */
+int dwcu_fft_c2r(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_out, int32_t device,
+                 void *stream);
+
+/* ---------------------------------------------------------------- timing */
+
+/* Per-kernel-class timing.  While enabled, every pass the engine launches
+ * is bracketed by CUDA events recorded on the stream it is launched on
+ * (inside CUDA graphs too).  dwcu_profile_collect waits for the recorded
+ * work, returns one entry per kernel class and clears the records.
+ * bytes_per_launch is the algorithmic HBM traffic of one launch (the bytes
+ * the pass must read and write), not a measured counter. */
+typedef struct dwcu_kernel_stat {
+    char name[40];
+    int64_t launches;
+    double milliseconds;      /* summed event time of all launches */
+    double bytes_per_launch;  /* algorithmic bytes of one launch */
+} dwcu_kernel_stat;
+int dwcu_profile_enable(int32_t on);
+int dwcu_profile_collect(dwcu_kernel_stat *stats, int32_t capacity, int32_t *count);
+
+/* ---------------------------------------------------------------- misc */
+
+/* Text of the last failure on this thread ("" if none). */
+const char *dwcu_last_error(void);
+/* ABI version, for the caller's check. */
+int dwcu_abi_version(void);
+/* Number of CUDA devices visible (0 without a GPU; never fails). */
+int dwcu_device_count(void);
+/* Number of kernel launches this thread has issued through the library. */
+int64_t dwcu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DWCU_H */

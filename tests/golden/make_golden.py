@@ -1,0 +1,78 @@
+"""Make the golden fixtures of the parity tests from the reference build.
+
+Every fixture here is produced by deconwolf's own method code (method_shb.c,
+method_rl.c, fft.c, fim.c compiled unmodified into oracle/_ref, see
+oracle/Makefile) on seeded synthetic inputs.  Run in a checkout that has the
+reference sources available to oracle/Makefile:
+
+    make -C oracle && python tests/golden/make_golden.py [--config1]
+
+Small fixtures store inputs and full outputs.  The 256 x 256 x 40 fixture
+(--config1, a few minutes of CPU) stores the I-divergence trace, per-plane
+sums and a seeded sample of 65536 output voxels; the inputs are regenerated
+from their seeds by deconwolf_b200.synthetic.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import pyoracle as po  # noqa: E402
+from tests.helpers import gauss_psf, poisson_image  # noqa: E402
+
+
+def small(name, shape, psf_shape, seed, **opts):
+    psf = gauss_psf(psf_shape, (1.3, 1.6, 1.9), seed=seed, jitter=0.15)
+    im = poisson_image(shape, psf, seed=seed, bg=80.0, npts=25)
+    r = po.deconvolve(im, psf, impl="reference", threads=os.cpu_count(), **opts)
+    out = {"image": im, "psf": psf, "out": r.out, "trace": r.trace, "iterations": np.int64(r.iterations),
+           "bg": np.float32(r.bg)}
+    for k, v in opts.items():
+        out["opt_" + k] = np.asarray(v)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, r.iterations, r.trace[:3])
+
+
+def sample_index(shape, n, seed=12345):
+    rng = np.random.default_rng(seed)
+    return rng.choice(int(np.prod(shape)), size=n, replace=False)
+
+
+def config1():
+    from deconwolf_b200 import synthetic
+    name = "shb-256x256x40"
+    im, psf = synthetic.config_inputs(name)
+    t = time.time()
+    r = po.deconvolve(im, psf, method="shb", n_iter=50, impl="reference", threads=os.cpu_count())
+    print("reference SHB 256x256x40, 50 it:", time.time() - t, "s; loop", r.loop_seconds)
+    idx = sample_index(im.shape, 65536)
+    np.savez_compressed(
+        os.path.join(HERE, "config1_shb50.npz"),
+        trace=r.trace, plane_sums=r.out.astype(np.float64).sum(axis=(1, 2)), sample_idx=idx,
+        sample_val=r.out.reshape(-1)[idx], norm=np.float64(np.linalg.norm(r.out.astype(np.float64))),
+        image_sum=np.float64(im.astype(np.float64).sum()), psf_sum=np.float64(psf.astype(np.float64).sum()),
+        image_sample=im.reshape(-1)[idx], bg=np.float32(r.bg), loop_seconds=np.float64(r.loop_seconds),
+        threads=np.int64(os.cpu_count()))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config1", action="store_true")
+    a = ap.parse_args()
+    small("small_shb", (11, 40, 37), (7, 9, 11), seed=11, method="shb", n_iter=20)
+    small("small_rl", (11, 40, 37), (7, 9, 11), seed=12, method="rl", n_iter=20)
+    small("small_shb_rel", (8, 33, 30), (5, 9, 9), seed=13, method="shb", iter_type=po.ITER_REL, err_rel=0.001)
+    if a.config1:
+        config1()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,214 @@
+"""GPU parity tests: the sm_100a engine, called through the C ABI, against
+the oracle (tests-only CPU checker).
+
+Tolerances (FP32 arithmetic, as in the reference):
+  * against the reference at its own job size: relative L2 of the output
+    <= 1e-4 and relative error of every I-divergence value <= 1e-5;
+  * against the oracle run at the same padded job size as the GPU (which
+    isolates FFT rounding): the same bounds, usually met by a wide margin.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import deconwolf_b200 as dw
+from oracle import pyoracle as po
+from tests.helpers import gauss_psf, poisson_image, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+OUT_TOL = 1e-4
+TRACE_TOL = 1e-5
+
+
+def trace_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.abs(b)))
+
+
+def case_inputs(seed=1, shape=(9, 22, 19), psf_shape=(5, 7, 9)):
+    psf = gauss_psf(psf_shape, (1.2, 1.5, 1.7), seed=seed, jitter=0.2)
+    im = poisson_image(shape, psf, seed=seed, bg=50.0, npts=15)
+    return im, psf
+
+
+def checker(**kw):
+    return "reference" if po.available("reference") else "port"
+
+
+CASES = [
+    dict(method="shb", n_iter=12),
+    dict(method="rl", n_iter=12),
+    dict(method="shb", n_iter=30),
+    dict(method="shb", iter_type=po.ITER_REL, err_rel=0.002),
+    dict(method="rl", iter_type=po.ITER_REL, err_rel=0.002),
+    dict(method="shb", iter_type=po.ITER_ABS, err_abs=1.5, maxiter=30),
+    dict(method="shb", n_iter=6, start=po.START_IDENTITY),
+    dict(method="rl", n_iter=6, metric=po.METRIC_MSE),
+    dict(method="shb", n_iter=6, bg=3.0, positivity=False),
+    dict(method="shb", n_iter=8, alphamax=0.3),
+    dict(method="rl", n_iter=5, bg=0.5),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}={v}" for k, v in c.items()))
+def test_method_matches_oracle(case):
+    im, psf = case_inputs()
+    g = dw.run_method(im, psf, **case)
+    # same padded job size as the GPU
+    p = po.deconvolve(im, psf, work=g.work, **case)
+    assert g.iterations == p.iterations
+    assert rel_l2(g.out, p.out) < OUT_TOL
+    assert trace_err(g.trace, p.trace) < TRACE_TOL
+    # the reference at its own job size
+    r = po.deconvolve(im, psf, impl=checker(), **case)
+    assert g.iterations == r.iterations
+    assert rel_l2(g.out, r.out) < OUT_TOL
+    assert trace_err(g.trace, r.trace) < TRACE_TOL
+    assert abs(g.bg - r.bg) <= 1e-6 * max(1.0, abs(r.bg))
+
+
+@pytest.mark.parametrize("shape,psf_shape,bq", [
+    ((1, 30, 26), (1, 7, 9), 2),        # 2-D image: z length 1
+    ((6, 17, 31), (3, 5, 5), 2),        # odd sizes
+    ((20, 50, 60), (7, 7, 7), 1),       # bq 1 on an exact supported job 64 x 54 x 24
+    ((16, 60, 60), (9, 9, 9), 0),       # bq 0: job = image size 60 x 60 x 16
+    ((5, 40, 3), (5, 9, 3), 2),         # thin x
+])
+def test_shapes_and_border_quality(shape, psf_shape, bq):
+    im, psf = case_inputs(seed=4, shape=shape, psf_shape=psf_shape)
+    for m in ("shb", "rl"):
+        g = dw.run_method(im, psf, method=m, n_iter=10, border_quality=bq)
+        r = po.deconvolve(im, psf, method=m, n_iter=10, border_quality=bq, impl=checker())
+        assert rel_l2(g.out, r.out) < OUT_TOL, m
+        assert trace_err(g.trace, r.trace) < TRACE_TOL, m
+
+
+def test_identity_and_first_iteration():
+    im, psf = case_inputs()
+    np.testing.assert_array_equal(dw.run_method(im, psf, n_iter=0).out, im)
+    g = dw.run_method(im, psf, method="shb", n_iter=1)
+    r = po.deconvolve(im, psf, method="shb", n_iter=1, impl=checker())
+    np.testing.assert_array_equal(g.out, r.out)  # the flat start, bit for bit
+
+
+@pytest.mark.parametrize("name", ["small_shb", "small_rl", "small_shb_rel"])
+def test_golden_fixtures(name):
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", f"{name}.npz"))
+    kw = {k[4:]: (v.item() if v.ndim == 0 else v) for k, v in d.items() if k.startswith("opt_")}
+    g = dw.run_method(d["image"], d["psf"], **kw)
+    assert g.iterations == int(d["iterations"])
+    assert rel_l2(g.out, d["out"]) < OUT_TOL
+    assert trace_err(g.trace, d["trace"]) < TRACE_TOL
+
+
+def test_config1_golden():
+    """256 x 256 x 40, Born-Wolf 127 x 127 x 79 PSF, SHB 50 iterations against
+    the reference's own output (sampled voxels, plane sums, full trace)."""
+    f = os.path.join(os.path.dirname(__file__), "golden", "config1_shb50.npz")
+    if not os.path.exists(f):
+        pytest.skip("config1 fixture not generated")
+    from deconwolf_b200 import synthetic
+    d = np.load(f)
+    im, psf = synthetic.config_inputs("shb-256x256x40")
+    idx = d["sample_idx"]
+    np.testing.assert_array_equal(im.reshape(-1)[idx], d["image_sample"])  # same inputs as the fixture
+    g = dw.run_method(im, psf, method="shb", n_iter=50)
+    assert g.work == (384, 384, 120)
+    assert trace_err(g.trace, d["trace"]) < TRACE_TOL
+    assert rel_l2(g.out.reshape(-1)[idx], d["sample_val"]) < OUT_TOL
+    assert rel_l2(g.out.astype(np.float64).sum(axis=(1, 2)), d["plane_sums"]) < OUT_TOL
+    assert abs(np.linalg.norm(g.out.astype(np.float64)) / d["norm"] - 1) < OUT_TOL
+
+
+def test_deterministic():
+    im, psf = case_inputs(seed=7, shape=(12, 40, 36), psf_shape=(7, 9, 9))
+    a = dw.run_method(im, psf, n_iter=15)
+    b = dw.run_method(im, psf, n_iter=15)
+    np.testing.assert_array_equal(a.out, b.out)
+    np.testing.assert_array_equal(a.trace, b.trace)
+
+
+def test_graph_and_eager_agree():
+    im, psf = case_inputs(seed=8, shape=(12, 40, 36), psf_shape=(7, 9, 9))
+    a = dw.run_method(im, psf, n_iter=9, use_graph=True)
+    b = dw.run_method(im, psf, n_iter=9, use_graph=False)
+    np.testing.assert_array_equal(a.out, b.out)
+
+
+def test_job_steps_equal_one_call():
+    im, psf = case_inputs(seed=9, shape=(10, 30, 28), psf_shape=(5, 7, 7))
+    ref = dw.run_method(im, psf, n_iter=11)
+    job = dw.Job(im.shape, psf.shape, n_iter=11)
+    job.setup(im, psf)
+    left = 11
+    while left:
+        left = job.step(3)
+    r = job.result()
+    job.close()
+    np.testing.assert_array_equal(r.out, ref.out)
+    np.testing.assert_array_equal(r.trace, ref.trace)
+
+
+def test_device_api_equals_host_api():
+    import torch
+    im, psf = case_inputs(seed=10, shape=(10, 30, 28), psf_shape=(5, 7, 7))
+    ref = dw.run_method(im, psf, n_iter=7, method="rl")
+    d_im = torch.from_numpy(im).cuda()
+    d_psf = torch.from_numpy(psf).cuda()
+    d_out = torch.empty_like(d_im)
+    torch.cuda.synchronize()
+    res = dw.run_method_device(d_im.data_ptr(), d_psf.data_ptr(), d_out.data_ptr(), im.shape, psf.shape,
+                               n_iter=7, method="rl")
+    np.testing.assert_array_equal(d_out.cpu().numpy(), ref.out)
+    np.testing.assert_array_equal(res.trace, ref.trace)
+
+
+def test_input_errors():
+    im, psf = case_inputs()
+    bad = im.copy()
+    bad[1, 2, 3] = np.nan
+    with pytest.raises(dw.DwcuError) as e:
+        dw.run_method(bad, psf, n_iter=3)
+    assert e.value.code == 5
+    with pytest.raises(dw.DwcuError) as e:
+        dw.run_method(im, psf, n_iter=3, start=dw.START_LP)
+    assert e.value.code == 2
+    # the context is still usable afterwards
+    assert dw.run_method(im, psf, n_iter=2).iterations == 2
+
+
+# ---------------------------------------------------------------- FFT
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("shape", [(12, 20, 16), (5, 9, 14), (1, 1, 2240), (180, 6, 8), (7, 12, 384)])
+def test_fft_r2c_matches_oracle(shape):
+    import torch
+    rng = np.random.default_rng(3)
+    x = rng.random(shape).astype(np.float32)
+    P, N, M = shape
+    d_x = _dev(x)
+    d_X = torch.empty((P, N, M // 2 + 1), dtype=torch.complex64, device="cuda")
+    torch.cuda.synchronize()
+    dw.fft_r2c_device(d_x.data_ptr(), shape, d_X.data_ptr())
+    X = d_X.cpu().numpy()
+    ref = np.fft.rfftn(x.astype(np.float64))
+    assert np.max(np.abs(X - ref)) / np.max(np.abs(ref)) < 2e-6
+    # c2r(r2c(x)) / n == x (fft.c:708-780: max relative error < 1e-5)
+    d_y = torch.empty_like(d_x)
+    dw.fft_c2r_device(d_X.data_ptr(), shape, d_y.data_ptr())
+    y = d_y.cpu().numpy() / np.float32(P * N * M)
+    xx = x + 5  # the reference's KAT uses values in [5, 6]
+    d_x2 = _dev(xx.astype(np.float32))
+    dw.fft_r2c_device(d_x2.data_ptr(), shape, d_X.data_ptr())
+    dw.fft_c2r_device(d_X.data_ptr(), shape, d_y.data_ptr())
+    y2 = d_y.cpu().numpy() / np.float32(P * N * M)
+    assert np.max(np.abs(y2 - xx) / xx) < 1e-5
+    assert np.max(np.abs(y - x)) < 1e-5
