@@ -112,12 +112,19 @@ struct ProfScope {
         rec.cls = prof_class(name, bytes);
         rec.a = prof_event();
         rec.b = prof_event();
-        cudaEventRecord(rec.a, st);
+        // inside stream capture a plain record is only a dependency edge;
+        // the external flag makes it a timing node of the graph
+        cudaEventRecordWithFlags(rec.a, st, capturing(st) ? cudaEventRecordExternal : 0);
+    }
+    static bool capturing(cudaStream_t s)
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        return cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive;
     }
     ~ProfScope()
     {
         if (!on) return;
-        cudaEventRecord(rec.b, st);
+        cudaEventRecordWithFlags(rec.b, st, capturing(st) ? cudaEventRecordExternal : 0);
         std::lock_guard<std::mutex> lk(g_prof_mu);
         g_prof_recs.push_back(rec);
     }
@@ -160,11 +167,22 @@ struct Geometry {
     long long M, N, P, pM, pN, pP;
     long long wM, wN, wP;   // the reference's job size (method_shb.c:137-153)
     long long X, Y, Z;      // padded job size
-    long long XC;           // complex row pitch
-    long long GP;           // image row pitch
+    long long XP;           // real row pitch (X rounded up to a multiple of 4)
+    long long NKB;          // kx blocks of the spectrum layout (X/2+1 over KB)
+    long long GP;           // image row pitch (multiple of 4)
     const XPlan *xp;
     const LinesPlan *yp, *zp;
+    const YPlan *ytp;       // pipelined y pass when the tile fits shared memory
+    long long spec_elems() const { return Z * NKB * Y * KB; }
+    long long real_elems() const { return XP * Y * Z; }
 };
+
+static const YPlan *find_y(int n)
+{
+    for (const auto &p : kYPlans)
+        if (p.n == n) return &p;
+    return nullptr;
+}
 
 static int make_geometry(long long M, long long N, long long P, long long pM, long long pN, long long pP, int bq,
                          Geometry &g)
@@ -195,14 +213,17 @@ static int make_geometry(long long M, long long N, long long P, long long pM, lo
                     g.wM, g.wN, g.wP, bq);
     g.xp = find_x((int) (g.X / 2));
     g.yp = g.Y > 1 ? find_lines((int) g.Y) : nullptr;
-    g.zp = g.Z > 1 ? find_lines((int) g.Z) : nullptr;
-    if (!g.xp) return fail(DWCU_ERROR_UNSUPPORTED, "x length %lld unsupported", g.X);
-    g.XC = (g.X / 2 + 1 + 1) & ~1LL;
-    g.GP = (M + 1) & ~1LL;
+    g.zp = find_lines((int) g.Z);  // also for Z == 1: the z pass carries the OTF multiply
+    if (!g.xp || !g.zp) return fail(DWCU_ERROR_UNSUPPORTED, "x length %lld or z length %lld unsupported", g.X, g.Z);
+    g.XP = (g.X + 3) & ~3LL;
+    g.NKB = (g.X / 2 + 1 + KB - 1) / KB;
+    g.GP = (M + 3) & ~3LL;
+    g.ytp = g.Y > 1 ? find_y((int) g.Y) : nullptr;
     return DWCU_SUCCESS;
 }
 
-static long long x_blocks(const Geometry &g) { return (g.Y * g.Z + g.xp->R - 1) / g.xp->R; }
+// x-pass tiles (= error partials): R rows of one z plane
+static long long x_blocks(const Geometry &g) { return g.Z * ((g.Y + g.xp->R - 1) / g.xp->R); }
 
 // ------------------------------------------------------------ twiddles
 
@@ -372,14 +393,29 @@ static int launch_lines(dwcu_job *j, const LinesPlan *p, const float2 *tw, long 
 static int pass_y(dwcu_job *j, int mode, float2 *data)
 {
     const Geometry &g = j->g;
-    // lines along y: stride XC, outer = z planes, columns = X/2+1
-    return launch_lines(j, g.yp, j->tw_y, g.Y, g.XC, g.XC * g.Y, g.Z, g.X / 2 + 1, mode, data, "y");
+    if (g.Y == 1) return DWCU_SUCCESS;
+    if (g.ytp) {
+        // one contiguous tile per (z, kx block): 4 lines of Y elements
+        YArgs a;
+        a.data = data;
+        a.tw = j->tw_y;
+        a.err = &j->sc->flags;
+        a.ntiles = (int) (g.Z * g.NKB);
+        a.dir = (mode == LINES_INV) ? +1 : -1;
+        ProfScope ps(mode == LINES_INV ? "y_inv" : "y_fwd", 16.0 * (double) g.spec_elems(), j->stream);
+        g.ytp->launch(a, j->stream);
+        CHECK_LAUNCH();
+        return DWCU_SUCCESS;
+    }
+    // lines along y: 4 contiguous columns, stride KB, outer = (z, kx block)
+    return launch_lines(j, g.yp, j->tw_y, g.Y, KB, g.Y * KB, g.Z * g.NKB, KB, mode, data, "y");
 }
 static int pass_z(dwcu_job *j, int mode, float2 *data)
 {
     const Geometry &g = j->g;
-    // lines along z: stride XC*Y, outer = y rows, columns = X/2+1
-    return launch_lines(j, g.zp, j->tw_z, g.Z, g.XC * g.Y, g.XC, g.Y, g.X / 2 + 1, mode, data, "z");
+    // lines along z: every (kx block, y, kx) of a plane is a column; stride = plane
+    const long long plane = g.NKB * g.Y * KB;
+    return launch_lines(j, g.zp, j->tw_z, g.Z, plane, 0, 1, plane, mode, data, "z");
 }
 
 static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, const float *srcp, float *dst,
@@ -397,15 +433,16 @@ static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, con
     a.dst = dst;
     a.partial = j->partial;
     a.sc = j->sc;
-    a.XC = g.XC;
-    a.X = g.X;
+    a.err = &j->sc->flags;
+    a.X = g.XP;
     a.GP = g.GP;
+    a.nkb = (int) g.NKB;
+    a.ntiles = (int) j->nxb;
     a.Y = (int) g.Y;
     a.Z = (int) g.Z;
     a.M = (int) g.M;
     a.N = (int) g.N;
     a.P = (int) g.P;
-    a.nrows = (int) (g.Y * g.Z);
     a.op = op;
     a.r2c = r2c;
     a.metric = j->s.metric;
@@ -417,7 +454,7 @@ static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, con
     static const char *names[] = {"x_fwd_copy", "x_fwd_ones", "x_fwd_shbp", "x_ratio_shb", "x_ratio_rl",
                                   "x_error", "x_update_shb", "x_update_rl", "x_weights", "x_store"};
     const double C = 8.0 * (double) (g.X / 2 + 1) * (double) (g.Y * g.Z);
-    const double R = 4.0 * (double) g.X * (double) (g.Y * g.Z);
+    const double R = 4.0 * (double) g.X * (double) (g.Y * g.Z);  // algorithmic: the X used columns
     const double G = 4.0 * (double) (g.M * g.N * g.P);
     static const double real_in[] = {1, 0, 2, 0, 0, 0, 3, 2, 0, 0};
     static const double real_out[] = {0, 0, 0, 0, 0, 0, 1, 1, 1, 1};
@@ -426,7 +463,7 @@ static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, con
     if (op == XOP_UPDATE_RL && !j->W) bytes -= R;
     if (op == XOP_RATIO_SHB || op == XOP_RATIO_RL || op == XOP_ERROR_ONLY) bytes += G;
     ProfScope ps(names[op], bytes, j->stream);
-    g.xp->launch(a, (int) j->nxb, j->stream);
+    g.xp->launch(a, j->stream);
     CHECK_LAUNCH();
     return DWCU_SUCCESS;
 }
@@ -501,9 +538,11 @@ static int iter_input(dwcu_job *j, int k)
 static int alloc_job(dwcu_job *j)
 {
     const Geometry &g = j->g;
-    const size_t R = sizeof(float) * (size_t) (g.X * g.Y * g.Z);
-    const size_t C = sizeof(float2) * (size_t) (g.XC * g.Y * g.Z);
-    const size_t G = sizeof(float) * (size_t) (g.GP * g.N * g.P);
+    // the x pass stages R rows per tile; a partial last tile reads (and
+    // never uses) one row past the end, so every staged array gets a spare row
+    const size_t R = sizeof(float) * (size_t) (g.real_elems() + g.XP);
+    const size_t C = sizeof(float2) * (size_t) (g.spec_elems() + 8 * KB);
+    const size_t G = sizeof(float) * (size_t) (g.GP * g.N * g.P + g.GP);
     j->nxb = x_blocks(g);
     j->n_spart = (int) std::min<long long>(1024, g.N * g.P);
     const long long npsf = g.pM * g.pN * g.pP;
@@ -547,8 +586,8 @@ static int alloc_job(dwcu_job *j)
 
 static long long job_bytes_estimate(const Geometry &g, const dwcu_opts &s)
 {
-    const long long R = 4LL * g.X * g.Y * g.Z;
-    const long long C = 8LL * g.XC * g.Y * g.Z;
+    const long long R = 4LL * g.real_elems();
+    const long long C = 8LL * g.spec_elems();
     const long long G = 4LL * g.GP * g.N * g.P;
     return G + 2 * C + (s.border_quality > 0 ? 3 : 2) * R + 8LL * ((g.Y * g.Z) / 2 + 1) +
            4LL * g.pM * g.pN * g.pP + (1 << 20);
@@ -589,7 +628,7 @@ static int job_create(long long M, long long N, long long P, long long pM, long 
     if (rc == DWCU_SUCCESS) rc = get_twiddles(ctx, g.X, &j->tw_x);
     if (rc == DWCU_SUCCESS) rc = get_twiddles(ctx, g.X / 2, &j->tw_l);
     if (rc == DWCU_SUCCESS && g.Y > 1) rc = get_twiddles(ctx, g.Y, &j->tw_y);
-    if (rc == DWCU_SUCCESS && g.Z > 1) rc = get_twiddles(ctx, g.Z, &j->tw_z);
+    if (rc == DWCU_SUCCESS) rc = get_twiddles(ctx, g.Z, &j->tw_z);
     if (rc == DWCU_SUCCESS && cudaMallocHost(&j->h_err, sizeof(float)) != cudaSuccess)
         rc = fail(DWCU_ERROR_OUT_OF_MEMORY, "pinned allocation failed");
     if (rc == DWCU_SUCCESS &&
@@ -637,11 +676,14 @@ static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_dev
     CHECK_LAUNCH();
     k_argmax_final<<<1, 32, 0, st>>>(j->apart, nab, j->amax);
     CHECK_LAUNCH();
-    const size_t R = sizeof(float) * (size_t) (g.X * g.Y * g.Z);
+    const size_t R = sizeof(float) * (size_t) g.real_elems();
+    CU(cudaMemsetAsync(j->S, 0, sizeof(float2) * (size_t) g.spec_elems(), st));
+    CU(cudaMemsetAsync(j->K, 0, sizeof(float2) * (size_t) g.spec_elems(), st));
     CU(cudaMemsetAsync(j->xb, 0, R, st));
     const float scale = (float) (1.0 / ((double) g.X * (double) g.Y * (double) g.Z));
     k_psf_embed<<<(int) std::min<long long>(4096, (npsf + 255) / 256), 256, 0, st>>>(
-        j->psf_dev, (int) g.pM, (int) g.pN, (int) g.pP, j->amax, j->xb, (int) g.X, (int) g.Y, (int) g.Z, scale);
+        j->psf_dev, (int) g.pM, (int) g.pN, (int) g.pP, j->amax, j->xb, (int) g.X, (int) g.Y, (int) g.Z,
+        (int) g.XP, scale);
     CHECK_LAUNCH();
     TRY(pass_x(j, XOP_FWD_COPY, 1, j->K, j->xb, nullptr, nullptr, 0, 0));
     TRY(pass_y(j, LINES_FWD, j->K));
@@ -655,14 +697,14 @@ static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_dev
     }
 
     // start estimate (method_shb.c:264-276); x_{-1} = x_0
-    const long long nv = g.X * g.Y * g.Z;
+    const long long nv = g.real_elems();
     const int fb = (int) std::min<long long>(148 * 16, (nv + 255) / 256);
     if (j->s.start_condition == DWCU_START_FLAT) {
         k_fill_scalar<<<fb, 256, 0, st>>>(j->xa, nv, j->sc);
         CHECK_LAUNCH();
     } else {
         CU(cudaMemsetAsync(j->xa, 0, R, st));
-        k_embed_image<<<fb, 256, 0, st>>>(j->gimg, g.GP, (int) g.M, (int) g.N, (int) g.P, j->xa, (int) g.X,
+        k_embed_image<<<fb, 256, 0, st>>>(j->gimg, g.GP, (int) g.M, (int) g.N, (int) g.P, j->xa, (int) g.XP,
                                           (int) g.Y);
         CHECK_LAUNCH();
     }
@@ -789,14 +831,17 @@ static int job_result(dwcu_job *j, float *out, bool on_device, dwcu_opts *so)
     }
     const long long n = g.M * g.N * g.P;
     const int fb = (int) std::min<long long>(148 * 16, (n + 255) / 256);
-    k_crop<<<fb, 256, 0, st>>>(j->xa, (int) g.X, (int) g.Y, (int) g.M, (int) g.N, (int) g.P, dout);
+    k_crop<<<fb, 256, 0, st>>>(j->xa, (int) g.XP, (int) g.Y, (int) g.M, (int) g.N, (int) g.P, dout);
     CHECK_LAUNCH();
     CU(cudaEventRecord(j->ev2, st));
     if (!on_device) CU(cudaMemcpyAsync(out, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
     const int nerr = j->done_iters;
     std::vector<float> errs((size_t) std::max(1, nerr));
     if (nerr > 0) CU(cudaMemcpyAsync(errs.data(), j->err, sizeof(float) * nerr, cudaMemcpyDeviceToHost, st));
+    JobScalars hs{};
+    CU(cudaMemcpyAsync(&hs, j->sc, sizeof hs, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
+    if (hs.flags & ~3) return fail(DWCU_ERROR_TIMEOUT, "a bounded wait in a pass gave up (flags 0x%x)", hs.flags);
     if (so) {
         so->iterations_done = nerr;
         so->bg = j->s.bg;
@@ -859,11 +904,13 @@ static int fft3d(const float *d_in, long long M, long long N, long long P, float
     g.wM = g.X = M; g.wN = g.Y = N; g.wP = g.Z = P;
     g.xp = find_x((int) (M / 2));
     g.yp = N > 1 ? find_lines((int) N) : nullptr;
-    g.zp = P > 1 ? find_lines((int) P) : nullptr;
-    if (!g.xp || (N > 1 && !g.yp) || (P > 1 && !g.zp))
+    g.zp = find_lines((int) P);
+    g.ytp = N > 1 ? find_y((int) N) : nullptr;
+    if (!g.xp || (N > 1 && !g.yp) || !g.zp)
         return fail(DWCU_ERROR_UNSUPPORTED, "unsupported transform size %lld x %lld x %lld", M, N, P);
-    g.XC = (M / 2 + 1 + 1) & ~1LL;
-    g.GP = (M + 1) & ~1LL;
+    g.XP = (M + 3) & ~3LL;
+    g.NKB = (M / 2 + 1 + KB - 1) / KB;
+    g.GP = (M + 3) & ~3LL;
     j->s.metric = DWCU_METRIC_IDIV;
     j->s.positivity = 1;
     j->ctx = ctx;
@@ -872,40 +919,59 @@ static int fft3d(const float *d_in, long long M, long long N, long long P, float
     TRY(get_twiddles(ctx, g.X, &j->tw_x));
     TRY(get_twiddles(ctx, g.X / 2, &j->tw_l));
     if (N > 1) TRY(get_twiddles(ctx, N, &j->tw_y));
-    if (P > 1) TRY(get_twiddles(ctx, P, &j->tw_z));
-    const size_t C = sizeof(float2) * (size_t) (g.XC * N * P);
+    TRY(get_twiddles(ctx, P, &j->tw_z));
+    const size_t C = align256(sizeof(float2) * (size_t) (g.spec_elems() + 8 * KB));
+    const size_t R = align256(sizeof(float) * (size_t) (g.real_elems() + g.XP));
     void *tmp = nullptr;
-    CU(cudaMalloc(&tmp, C + sizeof(JobScalars) + 256));
+    CU(cudaMalloc(&tmp, C + R + 256));
     j->S = (float2 *) tmp;
-    j->sc = (JobScalars *) ((char *) tmp + align256(C));
+    float *real = (float *) ((char *) tmp + C);
+    j->sc = (JobScalars *) ((char *) tmp + C + R);
     j->K = nullptr;
     j->W = nullptr;
     j->partial = nullptr;
     int rc = DWCU_SUCCESS;
-    const size_t hw = sizeof(float2) * (size_t) (M / 2 + 1);
-    if (cudaMemsetAsync(j->sc, 0, sizeof(JobScalars), j->stream) != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "memset");
+    const long long H = M / 2 + 1;
+    const long long nspec = H * N * P;
+    const int fb = (int) std::min<long long>(148 * 16, (nspec + 255) / 256);
+    if (cudaMemsetAsync(tmp, 0, C + R + 256, j->stream) != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "memset");
     if (forward) {
-        if (rc == DWCU_SUCCESS) rc = pass_x(j, XOP_FWD_COPY, 1, j->S, d_in, nullptr, nullptr, 0, 0);
+        if (rc == DWCU_SUCCESS &&
+            cudaMemcpy2DAsync(real, sizeof(float) * g.XP, d_in, sizeof(float) * M, sizeof(float) * M, N * P,
+                              cudaMemcpyDeviceToDevice, j->stream) != cudaSuccess)
+            rc = fail(DWCU_ERROR_CUDA, "copy failed");
+        if (rc == DWCU_SUCCESS) rc = pass_x(j, XOP_FWD_COPY, 1, j->S, real, nullptr, nullptr, 0, 0);
         if (rc == DWCU_SUCCESS) rc = pass_y(j, LINES_FWD, j->S);
         if (rc == DWCU_SUCCESS) rc = pass_z(j, LINES_FWD, j->S);
-        if (rc == DWCU_SUCCESS && cudaMemcpy2DAsync(d_out, hw, j->S, sizeof(float2) * g.XC, hw, N * P,
-                                                    cudaMemcpyDeviceToDevice, j->stream) != cudaSuccess)
-            rc = fail(DWCU_ERROR_CUDA, "copy failed");
+        if (rc == DWCU_SUCCESS) {
+            k_spec_unpack<<<fb, 256, 0, j->stream>>>(j->S, (int) H, (int) N, (int) P, (int) g.NKB,
+                                                     reinterpret_cast<float2 *>(d_out));
+            ++g_launches;
+            if (cudaGetLastError() != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "unpack launch failed");
+        }
     } else {
-        if (cudaMemcpy2DAsync(j->S, sizeof(float2) * g.XC, d_in, hw, hw, N * P, cudaMemcpyDeviceToDevice,
-                              j->stream) != cudaSuccess)
-            rc = fail(DWCU_ERROR_CUDA, "copy failed");
+        k_spec_pack<<<fb, 256, 0, j->stream>>>(reinterpret_cast<const float2 *>(d_in), (int) H, (int) N, (int) P,
+                                               (int) g.NKB, j->S);
+        ++g_launches;
+        if (cudaGetLastError() != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "pack launch failed");
         if (rc == DWCU_SUCCESS) rc = pass_z(j, LINES_INV, j->S);
         if (rc == DWCU_SUCCESS) rc = pass_y(j, LINES_INV, j->S);
-        if (rc == DWCU_SUCCESS) rc = pass_x(j, XOP_STORE, 0, j->S, nullptr, nullptr, d_out, 0, 0);
+        if (rc == DWCU_SUCCESS) rc = pass_x(j, XOP_STORE, 0, j->S, nullptr, nullptr, real, 0, 0);
+        if (rc == DWCU_SUCCESS &&
+            cudaMemcpy2DAsync(d_out, sizeof(float) * M, real, sizeof(float) * g.XP, sizeof(float) * M, N * P,
+                              cudaMemcpyDeviceToDevice, j->stream) != cudaSuccess)
+            rc = fail(DWCU_ERROR_CUDA, "copy failed");
     }
     cudaError_t e = cudaStreamSynchronize(j->stream);
+    JobScalars hs{};
+    if (e == cudaSuccess) e = cudaMemcpy(&hs, j->sc, sizeof hs, cudaMemcpyDeviceToHost);
     cudaFree(tmp);
     j->base = nullptr;
     j->ev0 = j->ev1 = j->ev2 = nullptr;
     j->stream = nullptr;
     if (rc != DWCU_SUCCESS) return rc;
     if (e != cudaSuccess) return fail(DWCU_ERROR_CUDA, "transform failed: %s", cudaGetErrorString(e));
+    if (hs.flags & ~3) return fail(DWCU_ERROR_TIMEOUT, "a bounded wait in a pass gave up (flags 0x%x)", hs.flags);
     return DWCU_SUCCESS;
 }
 

@@ -44,7 +44,7 @@ def tpl_of(n, s):
 def best_split(n):
     """(RA, RB, RC) with RA*RB*RC == n, radices in RADS (RB, RC may be 1)."""
     if n == 1:
-        return None
+        return (1, 1, 1)  # identity; the z pass of a 2-D job still multiplies by the OTF
     cands = []
     if n in RADS:
         cands.append((n, 1, 1))
@@ -86,23 +86,49 @@ def lines_T(n, split):
     return T, tpl
 
 
-def x_R(n, split):
-    """Rows per CTA for the x pass (complex half length n)."""
+SMEM_MAX = 220 * 1024
+KB = 4
+
+
+def padn(n, s):
+    return n + n // s[0] + 1
+
+
+def x_smem(n, split, R):
+    """Shared memory of k_xpass<RD, R> (mirrors XCfg in passes.cuh)."""
     a, b, c = split
     rev = (c, b, a) if c > 1 else (b, a, 1)
     tpl = max(tpl_of(n, split), tpl_of(n, rev))
-    row = (max(n + 1, n + n // min(a, rev[0]) + 1)) | 1
-    R = 1
-    while (2 * R) * tpl <= 512 and (2 * R) * row * 8 <= 48 * 1024 and R < 8:
+    threads = R * tpl
+    row = max(n + 1, padn(n, split), padn(n, rev)) | 1
+    nkb = (n + 1 + KB - 1) // KB
+    area = (max(R * nkb * KB, R * row) + 1) // 2 * 2
+    return 64 + 8 * area + 3 * 4 * R * ((2 * n + 3) // 4 * 4) + 8 * threads
+
+
+def x_R(n, split):
+    """Rows per x tile (complex half length n).  Two rows share each thread;
+    small rows take more thread rows so that a CTA has a full warp; the tile
+    should let three CTAs share an SM."""
+    a, b, c = split
+    rev = (c, b, a) if c > 1 else (b, a, 1)
+    tpl = max(tpl_of(n, split), tpl_of(n, rev))
+    R = 2
+    while R * tpl < 64:
         R *= 2
-    while R * tpl < 32:
-        R *= 2
+    while R > 1 and (3 * x_smem(n, split, R) > 225 * 1024 or R * tpl > 1024):
+        R //= 2
     return R, tpl
 
 
-def supported(maxn):
+def y_fits(n, split):
+    """k_ypass<RD> (4 lines, double buffered) fits in shared memory."""
+    return 2 * padn(n, split) * KB * 8 + 64 <= SMEM_MAX and KB * tpl_of(n, split) <= 1024
+
+
+def supported(maxn, start=2):
     out = []
-    for n in range(2, maxn + 1):
+    for n in range(start, maxn + 1):
         if smooth(n) and best_split(n):
             out.append(n)
     return out
@@ -120,11 +146,11 @@ def main():
     ap.add_argument("--only", type=str, default="", help="comma list of lengths (development builds)")
     args = ap.parse_args()
 
-    lines_ns = supported(args.max)
-    x_ns = supported(args.xmax)
+    lines_ns = supported(args.max, start=1)
+    x_ns = [n for n in supported(args.xmax) if x_smem(n, best_split(n), x_R(n, best_split(n))[0]) <= SMEM_MAX]
     if args.only:
         keep = {int(v) for v in args.only.split(",")}
-        lines_ns = [n for n in lines_ns if n in keep]
+        lines_ns = [n for n in lines_ns if n in keep or n == 1]
         x_ns = [n for n in x_ns if n in keep]
 
     hdr = []
@@ -133,13 +159,17 @@ def main():
     hdr.append("#include \"passes.cuh\"")
     hdr.append("namespace dwcu {")
     hdr.append("struct LinesPlan { int n, ra, rb, rc, T, threads; size_t smem; void (*launch)(const LinesArgs &, int, cudaStream_t); };")
-    hdr.append("struct XPlan { int n, ra, rb, rc, R, threads; size_t smem; void (*launch)(const XArgs &, int, cudaStream_t); };")
+    hdr.append("struct XPlan { int n, ra, rb, rc, R, threads; size_t smem; void (*launch)(const XArgs &, cudaStream_t); };")
+    hdr.append("struct YPlan { int n, ra, rb, rc, threads; size_t smem; void (*launch)(const YArgs &, cudaStream_t); };")
+    y_ns = [n for n in lines_ns if n > 1 and y_fits(n, best_split(n))]
     for n in lines_ns:
         s = best_split(n)
         T, _ = lines_T(n, s)
         hdr.append(f"void launch_lines_{n}(const LinesArgs &, int, cudaStream_t);")
     for n in x_ns:
-        hdr.append(f"void launch_x_{n}(const XArgs &, int, cudaStream_t);")
+        hdr.append(f"void launch_x_{n}(const XArgs &, cudaStream_t);")
+    for n in y_ns:
+        hdr.append(f"void launch_y_{n}(const YArgs &, cudaStream_t);")
     hdr.append("static const LinesPlan kLinesPlans[] = {")
     for n in lines_ns:
         s = best_split(n)
@@ -154,6 +184,12 @@ def main():
         hdr.append(f"    {{{n}, {s[0]}, {s[1]}, {s[2]}, {R}, XCfg<{rad_str(s)}, {R}>::THREADS, "
                    f"XCfg<{rad_str(s)}, {R}>::SMEM_BYTES, launch_x_{n}}},")
     hdr.append("};")
+    hdr.append("static const YPlan kYPlans[] = {")
+    for n in y_ns:
+        s_ = best_split(n)
+        hdr.append(f"    {{{n}, {s_[0]}, {s_[1]}, {s_[2]}, YCfg<{rad_str(s_)}>::THREADS, "
+                   f"YCfg<{rad_str(s_)}>::SMEM_BYTES, launch_y_{n}}},")
+    hdr.append("};")
     hdr.append("}  // namespace dwcu")
     with open(os.path.join(HERE, "plans_gen.h"), "w") as f:
         f.write("\n".join(hdr) + "\n")
@@ -163,7 +199,7 @@ def main():
         if old.startswith("inst_") and old.endswith(".cu"):
             os.remove(os.path.join(HERE, old))
     parts = max(1, args.parts)
-    for kind, ns in (("lines", lines_ns), ("x", x_ns)):
+    for kind, ns in (("lines", lines_ns), ("x", x_ns), ("y", y_ns)):
         for p in range(parts):
             chunk = ns[p::parts]
             lines = ["// generated by gen_plans.py -- do not edit", "#include \"launch.cuh\"", "namespace dwcu {"]
@@ -173,14 +209,17 @@ def main():
                     T, _ = lines_T(n, s)
                     lines.append(f"void launch_lines_{n}(const LinesArgs &a, int nb, cudaStream_t st) "
                                  f"{{ launch_lines_t<{rad_str(s)}, {T}>(a, nb, st); }}")
-                else:
+                elif kind == "x":
                     R, _ = x_R(n, s)
-                    lines.append(f"void launch_x_{n}(const XArgs &a, int nb, cudaStream_t st) "
-                                 f"{{ launch_x_t<{rad_str(s)}, {R}>(a, nb, st); }}")
+                    lines.append(f"void launch_x_{n}(const XArgs &a, cudaStream_t st) "
+                                 f"{{ launch_x_t<{rad_str(s)}, {R}>(a, st); }}")
+                else:
+                    lines.append(f"void launch_y_{n}(const YArgs &a, cudaStream_t st) "
+                                 f"{{ launch_y_t<{rad_str(s)}>(a, st); }}")
             lines.append("}  // namespace dwcu")
             with open(os.path.join(HERE, f"inst_{kind}_{p}.cu"), "w") as f:
                 f.write("\n".join(lines) + "\n")
-    print(f"lines lengths: {len(lines_ns)}  x half-lengths: {len(x_ns)}")
+    print(f"lines lengths: {len(lines_ns)}  x half-lengths: {len(x_ns)}  y tiles: {len(y_ns)}")
 
 
 if __name__ == "__main__":

@@ -1,16 +1,16 @@
 // generated by gen_plans.py -- do not edit
 #include "launch.cuh"
 namespace dwcu {
-void launch_lines_12(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<4, 3, 1>, 16>(a, nb, st); }
-void launch_lines_42(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<7, 6, 1>, 16>(a, nb, st); }
-void launch_lines_90(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<10, 9, 1>, 16>(a, nb, st); }
-void launch_lines_160(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<16, 10, 1>, 16>(a, nb, st); }
-void launch_lines_250(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<10, 5, 5>, 16>(a, nb, st); }
-void launch_lines_378(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<9, 6, 7>, 16>(a, nb, st); }
-void launch_lines_525(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<15, 5, 7>, 8>(a, nb, st); }
-void launch_lines_735(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<15, 7, 7>, 8>(a, nb, st); }
-void launch_lines_1000(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<10, 10, 10>, 8>(a, nb, st); }
-void launch_lines_1350(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<15, 9, 10>, 4>(a, nb, st); }
-void launch_lines_1800(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<15, 10, 12>, 4>(a, nb, st); }
-void launch_lines_2688(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<16, 12, 14>, 4>(a, nb, st); }
+void launch_lines_10(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<5, 2, 1>, 16>(a, nb, st); }
+void launch_lines_40(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<8, 5, 1>, 16>(a, nb, st); }
+void launch_lines_84(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<12, 7, 1>, 16>(a, nb, st); }
+void launch_lines_150(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<15, 10, 1>, 16>(a, nb, st); }
+void launch_lines_245(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<7, 5, 7>, 16>(a, nb, st); }
+void launch_lines_375(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<15, 5, 5>, 8>(a, nb, st); }
+void launch_lines_512(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<8, 8, 8>, 16>(a, nb, st); }
+void launch_lines_729(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<9, 9, 9>, 8>(a, nb, st); }
+void launch_lines_980(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<14, 7, 10>, 4>(a, nb, st); }
+void launch_lines_1344(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<14, 8, 12>, 4>(a, nb, st); }
+void launch_lines_1792(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<16, 8, 14>, 4>(a, nb, st); }
+void launch_lines_2560(const LinesArgs &a, int nb, cudaStream_t st) { launch_lines_t<Rad<16, 10, 16>, 4>(a, nb, st); }
 }  // namespace dwcu

@@ -158,7 +158,7 @@ __global__ void k_argmax_final(const ArgmaxPartial *part, int nb, long long *out
 // fim.c:982-1057 by minus the argmax), scaled by `scale` (the inverse
 // transform normalisation 1/(X*Y*Z) is folded into the OTF here).
 __global__ void k_psf_embed(const float *__restrict__ psf, int pM, int pN, int pP, const long long *amax,
-                            float *__restrict__ dst, int X, int Y, int Z, float scale)
+                            float *__restrict__ dst, int X, int Y, int Z, int XP, float scale)
 {
     const long long n = (long long) pM * pN * pP;
     const long long am = *amax;
@@ -173,7 +173,7 @@ __global__ void k_psf_embed(const float *__restrict__ psf, int pM, int pN, int p
         int x = (a - aa) % X; if (x < 0) x += X;
         int y = (b - ab) % Y; if (y < 0) y += Y;
         int z = (c - ac) % Z; if (z < 0) z += Z;
-        dst[((long long) z * Y + y) * X + x] = psf[k] * scale;
+        dst[((long long) z * Y + y) * XP + x] = psf[k] * scale;
     }
 }
 
@@ -209,6 +209,33 @@ __global__ void k_crop(const float *__restrict__ x, int X, int Y, int M, int N, 
         const int b = (int) ((k - (long long) c * M * N) / M);
         const int a = (int) (k - (long long) c * M * N - (long long) b * M);
         out[k] = x[((long long) c * Y + b) * X + a];
+    }
+}
+
+// compact half-spectrum (kx fastest, H = X/2+1 per row) <-> blocked layout
+__global__ void k_spec_unpack(const float2 *__restrict__ S, int H, int Y, int Z, int nkb, float2 *__restrict__ out)
+{
+    const long long n = (long long) H * Y * Z;
+    for (long long k = blockIdx.x * (long long) blockDim.x + threadIdx.x; k < n;
+         k += (long long) gridDim.x * blockDim.x) {
+        const int kx = (int) (k % H);
+        const long long r = k / H;
+        const int y = (int) (r % Y);
+        const int z = (int) (r / Y);
+        out[k] = S[(((long long) z * nkb + kx / KB) * Y + y) * KB + kx % KB];
+    }
+}
+
+__global__ void k_spec_pack(const float2 *__restrict__ in, int H, int Y, int Z, int nkb, float2 *__restrict__ S)
+{
+    const long long n = (long long) H * Y * Z;
+    for (long long k = blockIdx.x * (long long) blockDim.x + threadIdx.x; k < n;
+         k += (long long) gridDim.x * blockDim.x) {
+        const int kx = (int) (k % H);
+        const long long r = k / H;
+        const int y = (int) (r % Y);
+        const int z = (int) (r / Y);
+        S[(((long long) z * nkb + kx / KB) * Y + y) * KB + kx % KB] = in[k];
     }
 }
 

@@ -28,6 +28,7 @@
 #pragma once
 #include <cstdint>
 #include "dft.cuh"
+#include "tma.cuh"
 
 namespace dwcu {
 
@@ -48,64 +49,105 @@ struct Rad {
     static __device__ __forceinline__ int pad(int idx) { return idx + idx / RA; }
 };
 
-// one Stockham butterfly: v[r] = x[j + r*N/R] on entry; twiddled by
-// W_{NS*R}^{r*(j mod NS)} and transformed; output r belongs at
-// (j/NS)*NS*R + j%NS + r*NS.
-template <int N, int NS, int R, int DIR>
-__device__ __forceinline__ void butterfly(float2 (&v)[R], int j, const float2 *__restrict__ tw)
+// Twiddles of one Stockham stage for butterfly index j: W_{NS*R}^{r*(j mod NS)},
+// r = 1 .. R-1, loaded from the length-N table.  They depend only on j, so a
+// stage's twiddles are loaded before the barrier that precedes the stage.
+template <int N, int NS, int R>
+__device__ __forceinline__ void stage_twiddles(float2 (&w)[R], int j, const float2 *__restrict__ tw)
 {
-    if constexpr (NS > 1) {
-        constexpr int step = N / (NS * R);
-        const int jm = j % NS;
+    constexpr int step = N / (NS * R);
+    const int u = (j % NS) * step;
 #pragma unroll
-        for (int r = 1; r < R; ++r) {
-            float2 w = __ldg(&tw[r * jm * step]);
-            v[r] = (DIR < 0) ? cmul(v[r], w) : cmulc(v[r], w);
-        }
-    }
-    Dft<R, DIR>::run(v);
+    for (int r = 1; r < R; ++r) w[r] = __ldg(&tw[r * u]);
 }
 
-// Full line transform.  On entry thread t (< N/RA) holds its first-stage
-// input v[r] = x[t + r*N/RA].  On exit thread t (< N/RL) holds
-// o[r] = X[t + r*N/RL].  smem(i) gives this line's exchange slot for padded
-// index i.  Contains __syncthreads(): call uniformly from the whole block;
-// the exchange tile may be reused by the caller only after another barrier.
-template <class RD, int DIR, class SM>
-__device__ __forceinline__ void line_fft(float2 (&v)[RD::RA], float2 (&o)[RD::RL], int t,
+// one Stockham butterfly on Q rows that share the butterfly index:
+// v[q][r] = x_q[j + r*N/R] on entry, multiplied by the stage twiddles w[r]
+// (unless NS == 1) and transformed; output r belongs at
+// (j/NS)*NS*R + j%NS + r*NS.
+template <int NS, int R, int DIR, int Q>
+__device__ __forceinline__ void butterfly(float2 (&v)[Q][R], const float2 (&w)[R])
+{
+    if constexpr (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r)
+#pragma unroll
+            for (int q = 0; q < Q; ++q) v[q][r] = (DIR < 0) ? cmul(v[q][r], w[r]) : cmulc(v[q][r], w[r]);
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Dft<R, DIR>::run(v[q]);
+}
+
+// Full line transform of Q rows per thread.  On entry thread t (< N/RA)
+// holds its first-stage inputs v[q][r] = x_q[t + r*N/RA].  On exit thread t
+// (< N/RL) holds o[q][r] = X_q[t + r*N/RL].  smem(q, i) is row q's exchange
+// slot for padded index i (RD::pad); every index a thread touches in a stage
+// is its base plus a compile-time multiple, so addressing is one add per
+// access.  Contains __syncthreads(): call uniformly from the whole block; the
+// exchange tiles may be reused by the caller only after another barrier.
+// PREF: load each stage's twiddles before the barrier that precedes the
+// stage (hides their latency; costs registers across the barrier).
+template <class RD, int DIR, int Q, bool PREF = false, class SM>
+__device__ __forceinline__ void line_fft(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
                                          const float2 *__restrict__ tw, SM smem)
 {
     constexpr int N = RD::N, RA = RD::RA, RB = RD::RB, RC = RD::RC;
+    constexpr int M2 = N / RB;  // stage-2 butterflies; read stride, a multiple of RA
+    // stage 1 writes t*RA + r  ->  padded t*(RA+1) + r
     if (t < N / RA) {
-        butterfly<N, 1, RA, DIR>(v, t, tw);
+        float2 none[RA];
+        butterfly<1, RA, DIR, Q>(v, none);
+        const int b1 = t * (RA + 1);
 #pragma unroll
-        for (int r = 0; r < RA; ++r) *smem(RD::pad(t * RA + r)) = v[r];
+        for (int q = 0; q < Q; ++q)
+#pragma unroll
+            for (int r = 0; r < RA; ++r) *smem(q, b1 + r) = v[q][r];
     }
+    float2 w2[RB];
+    if (PREF && t < M2) stage_twiddles<N, RA, RB>(w2, t, tw);
     __syncthreads();
     if constexpr (RD::THREE) {
-        float2 u[RB];
-        if (t < N / RB) {
+        constexpr int M3 = N / RC;
+        float2 u[Q][RB];
+        if (t < M2) {
+            const int b2 = RD::pad(t);
 #pragma unroll
-            for (int r = 0; r < RB; ++r) u[r] = *smem(RD::pad(t + r * (N / RB)));
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int r = 0; r < RB; ++r) u[q][r] = *smem(q, b2 + r * (M2 + M2 / RA));
         }
         __syncthreads();
-        if (t < N / RB) {
-            butterfly<N, RA, RB, DIR>(u, t, tw);
-            const int base = (t / RA) * RA * RB + t % RA;
+        if (t < M2) {
+            if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
+            butterfly<RA, RB, DIR, Q>(u, w2);
+            const int base = (t / RA) * RA * RB + t % RA;  // writes base + r*RA
+            const int b3 = base + base / RA;
 #pragma unroll
-            for (int r = 0; r < RB; ++r) *smem(RD::pad(base + r * RA)) = u[r];
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int r = 0; r < RB; ++r) *smem(q, b3 + r * (RA + 1)) = u[q][r];
         }
+        float2 w3[RC];
+        if (PREF && t < M3) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
         __syncthreads();
-        if (t < N / RC) {
+        if (t < M3) {
+            const int b4 = RD::pad(t);
 #pragma unroll
-            for (int r = 0; r < RC; ++r) o[r] = *smem(RD::pad(t + r * (N / RC)));
-            butterfly<N, RA * RB, RC, DIR>(o, t, tw);
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int r = 0; r < RC; ++r) o[q][r] = *smem(q, b4 + r * (M3 + M3 / RA));
+            if (!PREF) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
+            butterfly<RA * RB, RC, DIR, Q>(o, w3);
         }
     } else {
-        if (t < N / RB) {
+        if (t < M2) {
+            const int b2 = RD::pad(t);
 #pragma unroll
-            for (int r = 0; r < RB; ++r) o[r] = *smem(RD::pad(t + r * (N / RB)));
-            butterfly<N, RA, RB, DIR>(o, t, tw);
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int r = 0; r < RB; ++r) o[q][r] = *smem(q, b2 + r * (M2 + M2 / RA));
+            if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
+            butterfly<RA, RB, DIR, Q>(o, w2);
         }
     }
 }
@@ -133,10 +175,13 @@ struct LinesCfg {
     static constexpr int THREADS = T * cmax(RD::TPL, RevRad<RD>::TPL);
     static constexpr size_t SMEM_BYTES =
         sizeof(float2) * (size_t) cmax(RD::PADN, RevRad<RD>::PADN) * T;
+    // aim for three resident CTAs when threads and shared memory allow
+    static constexpr int MIN_BLOCKS =
+        (THREADS * 3 <= 2048 && SMEM_BYTES * 3 <= 225 * 1024) ? 3 : (THREADS * 2 <= 2048 ? 2 : 1);
 };
 
 template <class RD, int T>
-__global__ void __launch_bounds__(LinesCfg<RD, T>::THREADS)
+__global__ void __launch_bounds__(LinesCfg<RD, T>::THREADS, LinesCfg<RD, T>::MIN_BLOCKS)
 k_lines(LinesArgs a)
 {
     using RV = RevRad<RD>;
@@ -152,24 +197,24 @@ k_lines(LinesArgs a)
     float2 *base = a.data + off;
     const long long ls = a.line_stride;
     const int mode = a.mode;
-    auto smem = [&](int i) { return sm + (size_t) i * T + line; };
+    auto smem = [&](int, int i) { return sm + (size_t) i * T + line; };
 
-    float2 v[RD::RA];
+    float2 v[1][RD::RA];
     if (t < N / RD::RA) {
 #pragma unroll
         for (int r = 0; r < RD::RA; ++r)
-            v[r] = valid ? base[(long long) (t + r * (N / RD::RA)) * ls] : make_float2(0.f, 0.f);
+            v[0][r] = valid ? base[(long long) (t + r * (N / RD::RA)) * ls] : make_float2(0.f, 0.f);
     }
-    float2 o[RD::RL];
+    float2 o[1][RD::RL];
     if (mode == LINES_INV)
-        line_fft<RD, +1>(v, o, t, a.tw, smem);
+        line_fft<RD, +1, 1>(v, o, t, a.tw, smem);
     else
-        line_fft<RD, -1>(v, o, t, a.tw, smem);
+        line_fft<RD, -1, 1>(v, o, t, a.tw, smem);
     constexpr int SL = N / RD::RL;
     if (mode == LINES_FWD || mode == LINES_INV) {
         if (t < SL && valid) {
 #pragma unroll
-            for (int r = 0; r < RD::RL; ++r) base[(long long) (t + r * SL) * ls] = o[r];
+            for (int r = 0; r < RD::RL; ++r) base[(long long) (t + r * SL) * ls] = o[0][r];
         }
         return;
     }
@@ -179,16 +224,110 @@ k_lines(LinesArgs a)
 #pragma unroll
         for (int r = 0; r < RD::RL; ++r) {
             float2 q = __ldg(&h[(long long) (t + r * SL) * ls]);
-            o[r] = (mode == LINES_CONV) ? cmul(o[r], q) : cmulc(o[r], q);
+            o[0][r] = (mode == LINES_CONV) ? cmul(o[0][r], q) : cmulc(o[0][r], q);
         }
     }
     __syncthreads();  // the exchange tile is free again
-    float2 q[RV::RL];
-    line_fft<RV, +1>(o, q, t, a.tw, smem);
+    float2 q[1][RV::RL];
+    line_fft<RV, +1, 1>(o, q, t, a.tw, smem);
     constexpr int SQ = N / RV::RL;
     if (t < SQ && valid) {
 #pragma unroll
-        for (int r = 0; r < RV::RL; ++r) base[(long long) (t + r * SQ) * ls] = q[r];
+        for (int r = 0; r < RV::RL; ++r) base[(long long) (t + r * SQ) * ls] = q[0][r];
+    }
+}
+
+// ------------------------------------------------------------ spectrum layout
+//
+// The half-spectrum (kx < X/2+1) is stored blocked by KB = 4 along kx:
+//   element (kx, y, z) at  ((z * nkb + kx / KB) * Y + y) * KB + kx % KB
+// (nkb = ceil((X/2+1) / KB)).  A y line group (4 neighbouring kx) is then one
+// contiguous Y*32-byte block, a z line is strided by the plane size, and the
+// two rows y, y+1 of one kx block are 64 contiguous bytes for the x pass.
+constexpr int KB = 4;
+
+// ------------------------------------------------------------ k_ypass
+
+struct YArgs {
+    float2 *data;
+    const float2 *tw;   // tw[m] = exp(-2 pi i m / Y)
+    int *err;           // error flags (bounded waits)
+    int ntiles;         // Z * nkb
+    int dir;            // -1 forward, +1 inverse
+};
+
+template <class RD>
+struct YCfg {
+    static constexpr int Q = 1;                  // lines per thread
+    static constexpr int TX = KB / Q;            // threads across the 4 lines
+    static constexpr int THREADS = TX * RD::TPL;
+    static constexpr int BUF_F2 = RD::PADN * KB;
+    static constexpr size_t SMEM_BYTES = 2 * sizeof(float2) * (size_t) BUF_F2 + 64;
+    static constexpr uint32_t TILE_BYTES = (uint32_t) (RD::N * KB * sizeof(float2));
+};
+
+// Persistent y transform: one CTA loops over (z, kx-block) tiles; each tile
+// (4 lines of length Y, contiguous) arrives by one bulk copy, the next
+// tile's copy is in flight while this one is transformed.
+template <class RD, int DIR>
+__global__ void __launch_bounds__(YCfg<RD>::THREADS)
+k_ypass(YArgs a)
+{
+    using C = YCfg<RD>;
+    constexpr int N = RD::N;
+    constexpr int Q = C::Q;
+    extern __shared__ __align__(128) unsigned char ysm[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ysm);
+    float2 *bufs = reinterpret_cast<float2 *>(ysm + 64);
+    const int l0 = threadIdx.x * Q;  // this thread's first line in the tile
+    const int t = threadIdx.y;
+    const int tid = t * C::TX + threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    int tile = blockIdx.x;
+    if (tid == 0 && tile < a.ntiles) {
+        mbar_arrive_expect_tx(&bars[0], C::TILE_BYTES);
+        tma_load_1d(bufs, a.data + (size_t) tile * N * KB, C::TILE_BYTES, &bars[0]);
+    }
+    for (int it = 0; tile < a.ntiles; ++it, tile += gridDim.x) {
+        const int b = it & 1;
+        float2 *buf = bufs + (size_t) b * C::BUF_F2;
+        fence_proxy_async();  // this thread's accesses to the other buffer precede the next bulk copy into it
+        __syncthreads();      // the other buffer is no longer read
+        const int next = tile + gridDim.x;
+        if (tid == 0 && next < a.ntiles) {
+            fence_proxy_async();
+            mbar_arrive_expect_tx(&bars[b ^ 1], C::TILE_BYTES);
+            tma_load_1d(bufs + (size_t) (b ^ 1) * C::BUF_F2, a.data + (size_t) next * N * KB, C::TILE_BYTES,
+                        &bars[b ^ 1]);
+        }
+        if (!wait_all(&bars[b], (it >> 1) & 1, a.err, 1 << 8)) {
+            if (tid == 0 && next < a.ntiles) drain(&bars[b ^ 1], ((it + 1) >> 1) & 1);
+            return;
+        }
+        float2 v[Q][RD::RA];
+        if (t < N / RD::RA) {
+#pragma unroll
+            for (int r = 0; r < RD::RA; ++r)
+#pragma unroll
+                for (int q = 0; q < Q; ++q) v[q][r] = buf[(t + r * (N / RD::RA)) * KB + l0 + q];
+        }
+        __syncthreads();  // natural-order reads done; the buffer becomes the exchange tile
+        auto smem = [&](int q, int i) { return buf + (size_t) i * KB + l0 + q; };
+        float2 o[Q][RD::RL];
+        line_fft<RD, DIR, Q>(v, o, t, a.tw, smem);
+        constexpr int SL = N / RD::RL;
+        if (t < SL) {
+            float2 *dst = a.data + (size_t) tile * N * KB + l0;
+#pragma unroll
+            for (int r = 0; r < RD::RL; ++r)
+#pragma unroll
+                for (int q = 0; q < Q; ++q) dst[(size_t) (t + r * SL) * KB + q] = o[q][r];
+        }
     }
 }
 
@@ -212,11 +351,11 @@ struct JobScalars {
     float x0;        // flat start value
     double sumg;     // sum of the image in double
     float gmin;
-    int flags;       // bit 0: non-finite value in the image or PSF
+    int flags;       // bit 0/1: non-finite image/PSF; bits 8+: bounded waits that gave up
 };
 
 struct XArgs {
-    float2 *S;             // spectrum rows, pitch XC
+    float2 *S;             // spectrum (blocked layout)
     const float2 *tw;      // tw[m] = exp(-2 pi i m / X), m < X (Hermitian pre/post)
     const float2 *twL;     // twL[m] = exp(-2 pi i m / L), m < L (stage twiddles)
     const float *g;        // image, row pitch GP
@@ -224,14 +363,15 @@ struct XArgs {
     const float *srcp;     // x_{k-1} for SHB
     const float *Wt;       // Bertero weights (may be null)
     float *dst;            // real output (UPDATE: x_{k+1}; WEIGHTS/STORE)
-    double *partial;       // per-CTA error partials (ops with an error)
+    double *partial;       // per-tile error partials (ops with an error)
     const JobScalars *sc;  // bg, ...
-    long long XC;          // complex row pitch
-    long long X;           // real row pitch (= real length)
-    long long GP;
+    int *err;              // error flags (bounded waits)
+    long long X;           // real row pitch (= real length), multiple of 4
+    long long GP;          // image row pitch, multiple of 4
     int Y, Z;              // padded dims
     int M, N, P;           // image dims
-    int nrows;             // Y * Z
+    int nkb;               // kx blocks
+    int ntiles;            // Z * ceil(Y / R)
     int op;
     int r2c;               // run the forward transform after the op
     int metric;            // 1: I-divergence, 0: squared error
@@ -243,15 +383,35 @@ struct XArgs {
 
 // The x transform of a real row of X = 2L samples uses a complex transform
 // of length L = RD::N: z[n] = x[2n] + i x[2n+1].  The inverse runs with RD,
-// the forward with the reversed radix list.
+// the forward with the reversed radix list.  One CTA = one tile of R
+// consecutive rows (y0 .. y0+R-1 at one z).  At entry the CTA issues bulk
+// copies of its complex rows (the 64-byte kx blocks of the spectrum layout)
+// and, on a second barrier, of its real rows; the real rows arrive while the
+// inverse transform runs.  Three CTAs share an SM, so one CTA's copies
+// overlap the others' arithmetic.
 template <class RD, int R>
 struct XCfg {
     using RV = RevRad<RD>;
+    static constexpr int Q = 1;                     // rows per thread
+    static constexpr int RY = R / Q;                // thread rows of the block
     static constexpr int L = RD::N;
+    static constexpr int X = 2 * L;
+    static constexpr int XP = (X + 3) / 4 * 4;  // real row pitch (16-byte rows for bulk copies)
+    static constexpr int NKB = (L + 1 + KB - 1) / KB;
     static constexpr int TPL = cmax(RD::TPL, RV::TPL);
-    static constexpr int THREADS = R * TPL;
+    static constexpr int THREADS = RY * TPL;
     static constexpr int ROW_F2 = cmax(cmax(L + 1, RD::PADN), RV::PADN) | 1;
-    static constexpr size_t SMEM_BYTES = sizeof(float2) * (size_t) ROW_F2 * R + sizeof(double) * THREADS;
+    static constexpr int CPLX_F2 = R * NKB * KB;                  // staged rows, [kb][r][ki]
+    // complex area (also the exchange tiles), rounded to 16 bytes
+    static constexpr int AREA_F2 = (cmax(CPLX_F2, R * ROW_F2) + 1) / 2 * 2;
+    static constexpr int REAL_F = R * XP;                         // one staged real array
+    // complex area and three real slots: x (or the image rows g, which no op
+    // reads together with x), xp, W
+    static constexpr size_t REAL_OFF = 64 + sizeof(float2) * (size_t) AREA_F2;
+    static constexpr size_t RED_OFF = REAL_OFF + 3 * sizeof(float) * (size_t) REAL_F;
+    static constexpr size_t SMEM_BYTES = RED_OFF + sizeof(double) * THREADS;
+    static constexpr int MIN_BLOCKS = (SMEM_BYTES * 3 <= 225 * 1024 && THREADS * 3 <= 2048) ? 3 : 1;
+    static_assert(R % Q == 0, "rows per tile");
     static_assert(THREADS >= 32, "the error reduction needs one full warp");
 };
 
@@ -266,221 +426,344 @@ __device__ __forceinline__ double err_term(float yv, float gv, int metric)
 {
     double y = yv, g = gv;
     if (metric == 0) return (y - g) * (y - g);
-    // dw.c:1514-1517: g*logf(g/y) - (g - y) for y > 0 and g > 0
-    if (y > 0 && g > 0) return g * (double) logf((float) (g / y)) - (g - y);
+    // dw.c:1514-1517: g*logf(g/y) - (g - y) for y > 0 and g > 0.  The
+    // reference divides in double and rounds to float for logf; the float
+    // division gives the same float except in double-rounding ties.
+    if (yv > 0.f && gv > 0.f) return g * (double) logf(gv / yv) - (g - y);
     return 0.0;
 }
 
-// the pointwise op on the two real samples c0 = 2n, c0+1 of one row;
-// (y0, y1) are the C2R values (unused by the forward-only ops); returns the
-// two values handed to the forward transform
-__device__ __forceinline__ float2 x_op(const XArgs &a, int op, long long rbase, long long gbase, int c0,
-                                       bool img0, bool img1, float y0, float y1, float bg, double &acc)
+// ops are compiled in four families, one kernel each, so that every kernel's
+// code stays small: forward-only, ratio/error, update, and C2R-store ops
+enum XFam { XFAM_FWD = 0, XFAM_RATIO = 1, XFAM_UPDATE = 2, XFAM_STORE = 3 };
+__host__ __device__ constexpr int x_family(int op)
 {
-    float v0 = 0.f, v1 = 0.f;
+    return op <= XOP_FWD_SHBP ? XFAM_FWD
+         : op <= XOP_ERROR_ONLY ? XFAM_RATIO
+         : op <= XOP_UPDATE_RL ? XFAM_UPDATE : XFAM_STORE;
+}
+
+__device__ __forceinline__ bool op_c2r(int op) { return op >= XOP_RATIO_SHB; }
+__device__ __forceinline__ bool op_reads_x(int op)
+{
+    return op == XOP_FWD_COPY || op == XOP_FWD_SHBP || op == XOP_UPDATE_SHB || op == XOP_UPDATE_RL;
+}
+__device__ __forceinline__ bool op_reads_xp(int op) { return op == XOP_FWD_SHBP || op == XOP_UPDATE_SHB; }
+__device__ __forceinline__ bool op_reads_g(int op) { return op >= XOP_RATIO_SHB && op <= XOP_ERROR_ONLY; }
+
+// The pointwise op of one row: w[r] holds z[n] = (x[2n], x[2n+1]) for
+// n = t + r*SL -- the C2R output for the C2R ops -- and is replaced by the
+// values handed to the forward transform.  The row's real inputs are staged
+// in shared memory (sx: x or the image row, sxp: x_{k-1}, sw: weights).
+// The switch is outside the element loop so each op is one straight loop.
+template <int FAM, int RL, int SL>
+__device__ __forceinline__ void x_row_op(const XArgs &a, int op, int t, long long rbase, const float *sx,
+                                         const float *sxp, const float *sw, bool in_img_row, float bg,
+                                         float2 (&w)[RL], double &acc)
+{
+    const int M = a.M;
+    // only this family's cases are compiled into the kernel
+    if (x_family(op) != FAM) return;
     switch (op) {
-    case XOP_FWD_COPY: {
-        float2 s = *reinterpret_cast<const float2 *>(a.src + rbase + c0);
-        v0 = s.x; v1 = s.y;
-    } break;
-    case XOP_FWD_ONES:  // initial_guess, dw.c:2497-2520
-        v0 = img0 ? 1.f : 0.f;
-        v1 = img1 ? 1.f : 0.f;
+    case XOP_FWD_COPY:
+        if constexpr (FAM == XFAM_FWD) {
+#pragma unroll
+            for (int r = 0; r < RL; ++r) w[r] = *reinterpret_cast<const float2 *>(sx + 2 * (t + r * SL));
+        }
         break;
-    case XOP_FWD_SHBP: {
-        float2 xv = *reinterpret_cast<const float2 *>(a.src + rbase + c0);
-        float2 xq = *reinterpret_cast<const float2 *>(a.srcp + rbase + c0);
-        v0 = shb_p(xv.x, xq.x, a.alpha, bg);
-        v1 = shb_p(xv.y, xq.y, a.alpha, bg);
-    } break;
+    case XOP_FWD_ONES:  // initial_guess, dw.c:2497-2520
+        if constexpr (FAM == XFAM_FWD) {
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int c0 = 2 * (t + r * SL);
+                w[r] = make_float2(in_img_row && c0 < M ? 1.f : 0.f, in_img_row && c0 + 1 < M ? 1.f : 0.f);
+            }
+        }
+        break;
+    case XOP_FWD_SHBP:
+        if constexpr (FAM == XFAM_FWD) {
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int c0 = 2 * (t + r * SL);
+                const float2 xv = *reinterpret_cast<const float2 *>(sx + c0);
+                const float2 xq = *reinterpret_cast<const float2 *>(sxp + c0);
+                w[r] = make_float2(shb_p(xv.x, xq.x, a.alpha, bg), shb_p(xv.y, xq.y, a.alpha, bg));
+            }
+        }
+        break;
     case XOP_RATIO_SHB:
     case XOP_RATIO_RL:
-    case XOP_ERROR_ONLY: {
-        float g0 = 0.f, g1 = 0.f;
-        if (img1) {
-            float2 gg = *reinterpret_cast<const float2 *>(a.g + gbase + c0);
-            g0 = gg.x; g1 = gg.y;
-        } else if (img0) {
-            g0 = a.g[gbase + c0];
+    case XOP_ERROR_ONLY:
+        if constexpr (FAM != XFAM_RATIO) break;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const int c0 = 2 * (t + r * SL);
+            const bool img0 = in_img_row && c0 < M;
+            const bool img1 = in_img_row && c0 + 1 < M;
+            const float y0 = w[r].x, y1 = w[r].y;
+            const float g0 = img0 ? sx[c0] : 0.f;
+            const float g1 = img1 ? sx[c0 + 1] : 0.f;
+            if (img0) acc += err_term(y0, g0, a.metric);
+            if (img1) acc += err_term(y1, g1, a.metric);
+            float v0 = 0.f, v1 = 0.f;
+            if (op == XOP_RATIO_SHB) {
+                // method_shb.c:31-48: |y| < 1e-6 -> +-1e-6; r = g/y on the image, 0 elsewhere
+                float d0 = y0, d1 = y1;
+                if ((double) fabsf(d0) < 1e-6) d0 = copysignf(1e-6f, d0);
+                if ((double) fabsf(d1) < 1e-6) d1 = copysignf(1e-6f, d1);
+                v0 = img0 ? g0 / d0 : 0.f;
+                v1 = img1 ? g1 / d1 : 0.f;
+            } else if (op == XOP_RATIO_RL) {
+                // method_rl.c:46-67: r = g/y if y > 0 else bg on the image, 1e-6 elsewhere
+                v0 = img0 ? (y0 > 0.f ? g0 / y0 : bg) : 1e-6f;
+                v1 = img1 ? (y1 > 0.f ? g1 / y1 : bg) : 1e-6f;
+            }
+            w[r] = make_float2(v0, v1);
         }
-        if (img0) acc += err_term(y0, g0, a.metric);
-        if (img1) acc += err_term(y1, g1, a.metric);
-        if (op == XOP_RATIO_SHB) {
-            // method_shb.c:31-48: |y| < 1e-6 -> +-1e-6; r = g/y on the image, 0 elsewhere
-            float d0 = y0, d1 = y1;
-            if ((double) fabsf(d0) < 1e-6) d0 = copysignf(1e-6f, d0);
-            if ((double) fabsf(d1) < 1e-6) d1 = copysignf(1e-6f, d1);
-            v0 = img0 ? g0 / d0 : 0.f;
-            v1 = img1 ? g1 / d1 : 0.f;
-        } else if (op == XOP_RATIO_RL) {
-            // method_rl.c:46-67: r = g/y if y > 0 else bg on the image, 1e-6 elsewhere
-            v0 = img0 ? (y0 > 0.f ? g0 / y0 : bg) : 1e-6f;
-            v1 = img1 ? (y1 > 0.f ? g1 / y1 : bg) : 1e-6f;
-        }
-    } break;
-    case XOP_UPDATE_SHB: {
+        break;
+    case XOP_UPDATE_SHB:
         // method_shb.c:56-62 (x = Kt r * (p*W)), :366-376 (positivity), and the
         // next extrapolation :333-339; p_k is recomputed from x_k, x_{k-1}
-        float2 xv = *reinterpret_cast<const float2 *>(a.src + rbase + c0);
-        float2 xq = *reinterpret_cast<const float2 *>(a.srcp + rbase + c0);
-        float p0 = shb_p(xv.x, xq.x, a.alpha, bg);
-        float p1 = shb_p(xv.y, xq.y, a.alpha, bg);
-        float n0, n1;
-        if (a.Wt) {
-            float2 ww = *reinterpret_cast<const float2 *>(a.Wt + rbase + c0);
-            n0 = y0 * (p0 * ww.x);
-            n1 = y1 * (p1 * ww.y);
-        } else {
-            n0 = y0 * p0;
-            n1 = y1 * p1;
+        if constexpr (FAM != XFAM_UPDATE) break;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const int c0 = 2 * (t + r * SL);
+            const float2 xv = *reinterpret_cast<const float2 *>(sx + c0);
+            const float2 xq = *reinterpret_cast<const float2 *>(sxp + c0);
+            const float p0 = shb_p(xv.x, xq.x, a.alpha, bg);
+            const float p1 = shb_p(xv.y, xq.y, a.alpha, bg);
+            float n0, n1;
+            if (sw) {
+                const float2 ww = *reinterpret_cast<const float2 *>(sw + c0);
+                n0 = w[r].x * (p0 * ww.x);
+                n1 = w[r].y * (p1 * ww.y);
+            } else {
+                n0 = w[r].x * p0;
+                n1 = w[r].y * p1;
+            }
+            if (a.positivity) {
+                n0 = n0 < bg ? bg : n0;
+                n1 = n1 < bg ? bg : n1;
+            }
+            *reinterpret_cast<float2 *>(a.dst + rbase + c0) = make_float2(n0, n1);
+            w[r] = make_float2(shb_p(n0, xv.x, a.alpha_next, bg), shb_p(n1, xv.y, a.alpha_next, bg));
         }
-        if (a.positivity) {
-            n0 = n0 < bg ? bg : n0;
-            n1 = n1 < bg ? bg : n1;
-        }
-        *reinterpret_cast<float2 *>(a.dst + rbase + c0) = make_float2(n0, n1);
-        v0 = shb_p(n0, xv.x, a.alpha_next, bg);
-        v1 = shb_p(n1, xv.y, a.alpha_next, bg);
-    } break;
-    case XOP_UPDATE_RL: {
+        break;
+    case XOP_UPDATE_RL:
         // method_rl.c:84-98 and :362-372
-        float2 xv = *reinterpret_cast<const float2 *>(a.src + rbase + c0);
-        float n0, n1;
-        if (a.Wt) {
-            float2 ww = *reinterpret_cast<const float2 *>(a.Wt + rbase + c0);
-            n0 = y0 * (xv.x * ww.x);
-            n1 = y1 * (xv.y * ww.y);
-        } else {
-            n0 = y0 * xv.x;
-            n1 = y1 * xv.y;
+        if constexpr (FAM != XFAM_UPDATE) break;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const int c0 = 2 * (t + r * SL);
+            const float2 xv = *reinterpret_cast<const float2 *>(sx + c0);
+            float n0, n1;
+            if (sw) {
+                const float2 ww = *reinterpret_cast<const float2 *>(sw + c0);
+                n0 = w[r].x * (xv.x * ww.x);
+                n1 = w[r].y * (xv.y * ww.y);
+            } else {
+                n0 = w[r].x * xv.x;
+                n1 = w[r].y * xv.y;
+            }
+            if (a.rl_clamp && bg > 0.f) {
+                n0 = n0 < bg ? bg : n0;
+                n1 = n1 < bg ? bg : n1;
+            }
+            *reinterpret_cast<float2 *>(a.dst + rbase + c0) = make_float2(n0, n1);
+            w[r] = make_float2(n0, n1);
         }
-        if (a.rl_clamp && bg > 0.f) {
-            n0 = n0 < bg ? bg : n0;
-            n1 = n1 < bg ? bg : n1;
-        }
-        *reinterpret_cast<float2 *>(a.dst + rbase + c0) = make_float2(n0, n1);
-        v0 = n0;
-        v1 = n1;
-    } break;
-    case XOP_WEIGHTS: {
+        break;
+    case XOP_WEIGHTS:
         // method_shb.c:224-234: W = 1/P1 where P1 > 0.01, else 0
-        float q0 = y0 > 0.01f ? (float) (1.0 / (double) y0) : 0.f;
-        float q1 = y1 > 0.01f ? (float) (1.0 / (double) y1) : 0.f;
-        *reinterpret_cast<float2 *>(a.dst + rbase + c0) = make_float2(q0, q1);
-    } break;
+        if constexpr (FAM != XFAM_STORE) break;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const int c0 = 2 * (t + r * SL);
+            const float q0 = w[r].x > 0.01f ? (float) (1.0 / (double) w[r].x) : 0.f;
+            const float q1 = w[r].y > 0.01f ? (float) (1.0 / (double) w[r].y) : 0.f;
+            *reinterpret_cast<float2 *>(a.dst + rbase + c0) = make_float2(q0, q1);
+        }
+        break;
     case XOP_STORE:
-        *reinterpret_cast<float2 *>(a.dst + rbase + c0) = make_float2(y0, y1);
+        if constexpr (FAM == XFAM_STORE) {
+#pragma unroll
+            for (int r = 0; r < RL; ++r) *reinterpret_cast<float2 *>(a.dst + rbase + 2 * (t + r * SL)) = w[r];
+        }
         break;
     default:
         break;
     }
-    return make_float2(v0, v1);
 }
 
-template <class RD, int R>
-__global__ void __launch_bounds__(XCfg<RD, R>::THREADS)
+template <class RD, int R, int FAM>
+__global__ void __launch_bounds__(XCfg<RD, R>::THREADS, XCfg<RD, R>::MIN_BLOCKS)
 k_xpass(XArgs a)
 {
     using C = XCfg<RD, R>;
     using RV = typename C::RV;
     constexpr int L = C::L;
+    constexpr int Q = C::Q;
+    constexpr int XP = C::XP;       // real row pitch (a.X == XP)
     constexpr int SL = L / RD::RL;  // op phase: thread t < SL holds n = t + r*SL
     static_assert(RV::RA == RD::RL, "reversed radix list");
-    extern __shared__ float2 smx[];
+    extern __shared__ __align__(128) unsigned char xsm[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(xsm);  // [1]: real rows
+    float2 *CB = reinterpret_cast<float2 *>(xsm + 64);
+    float *RB = reinterpret_cast<float *>(xsm + C::REAL_OFF);
+    double *red = reinterpret_cast<double *>(xsm + C::RED_OFF);
     const int t = threadIdx.x;
-    const int rr = threadIdx.y;
-    const int row = blockIdx.x * R + rr;
-    const bool rvalid = row < a.nrows;
-    const int yy = rvalid ? row % a.Y : 0;
-    const int zz = rvalid ? row / a.Y : 0;
-    float2 *B = smx + (size_t) rr * C::ROW_F2;
-    float2 *Srow = a.S + (long long) row * a.XC;
+    const int ry = threadIdx.y;
+    const int tid = ry * C::TPL + t;
     const int op = a.op;
-    const bool c2r = (op >= XOP_RATIO_SHB);
-    const bool in_img_row = rvalid && yy < a.N && zz < a.P;
-    const float bg = a.sc->bg;
+    constexpr bool c2r = (FAM != XFAM_FWD);
+    const bool rx = op_reads_x(op), rxp = op_reads_xp(op), rw = rx && (op >= XOP_UPDATE_SHB) && a.Wt != nullptr;
+    constexpr bool rg = (FAM == XFAM_RATIO);
+    const int ytiles = (a.Y + R - 1) / R;
+    const long long plane = (long long) a.nkb * a.Y * KB;  // complex elements per z plane
+    const int tile = blockIdx.x;
+    const int z = tile / ytiles;
+    const int y0 = (tile - z * ytiles) * R;
+
+    // ---- bulk copies of this tile (warp 0)
+    const bool grow = rg && z < a.P && y0 < a.N;
+    const int gr = grow ? min(R, a.N - y0) : 0;
+    const uint32_t rbytes = (uint32_t) (R * XP * sizeof(float));
+    const uint32_t gbytes = (uint32_t) ((long long) gr * a.GP * sizeof(float));
+    const uint32_t cbytes = c2r ? (uint32_t) (C::NKB * R * KB * sizeof(float2)) : 0u;
+    const uint32_t real_total = rbytes * ((rx ? 1 : 0) + (rxp ? 1 : 0) + (rw ? 1 : 0)) + gbytes;
+    if (tid == 0) {
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    // complex rows: every kx block of this tile is R*32 contiguous bytes;
+    // 16-byte asynchronous copies spread over all threads
+    if constexpr (c2r) {
+        constexpr int PIECES = R * KB * (int) sizeof(float2) / 16;  // per kx block
+        const float4 *src = reinterpret_cast<const float4 *>(a.S + (long long) z * plane + (long long) y0 * KB);
+        float4 *dst = reinterpret_cast<float4 *>(CB);
+        const long long kstride = (long long) a.Y * KB * (long long) sizeof(float2) / 16;
+        for (int e = tid; e < C::NKB * PIECES; e += C::THREADS) {
+            const int kb = e / PIECES, p = e - kb * PIECES;
+            cp_async16(dst + e, src + kb * kstride + p);
+        }
+        cp_async_commit();
+    }
+    (void) cbytes;
+    __syncthreads();
+    if (tid < 32) {
+        if (tid == 0) mbar_arrive_expect_tx(&bars[1], real_total);
+        __syncwarp();
+        const long long row0 = (long long) z * a.Y + y0;
+        if (tid == 1 && rx) tma_load_1d(RB, a.src + row0 * XP, rbytes, &bars[1]);
+        if (tid == 2 && rxp) tma_load_1d(RB + C::REAL_F, a.srcp + row0 * XP, rbytes, &bars[1]);
+        if (tid == 3 && rw) tma_load_1d(RB + 2 * C::REAL_F, a.Wt + row0 * XP, rbytes, &bars[1]);
+        if (tid == 4 && gr > 0) tma_load_1d(RB, a.g + ((long long) z * a.N + y0) * a.GP, gbytes, &bars[1]);
+    }
+    // this thread's rows: ry*Q + q
+    auto smem = [&](int q, int i) { return CB + (size_t) (ry * Q + q) * C::ROW_F2 + i; };
     double acc = 0.0;
-    auto smem = [&](int i) { return B + i; };
+    const float bg = a.sc->bg;
 
-    float2 w[RD::RL];  // thread t < SL holds z[t + r*SL] = x[2n] + i x[2n+1]
+    float2 w[Q][RD::RL];  // thread t < SL holds z_q[t + r*SL] = x[2n] + i x[2n+1]
 #pragma unroll
-    for (int r = 0; r < RD::RL; ++r) w[r] = make_float2(0.f, 0.f);
+    for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < RD::RL; ++r) w[q][r] = make_float2(0.f, 0.f);
 
-    if (c2r) {
-        if (rvalid)
-            for (int k = t; k <= L; k += C::TPL) B[k] = Srow[k];
-        __syncthreads();
+    if constexpr (c2r) {
+        cp_async_wait_all();
+        __syncthreads();  // every thread's copies have landed
         // first-stage inputs Z[k] = (X[k] + X*[L-k]) + i W_X^{-k} (X[k] - X*[L-k]);
         // Im X[0] and Im X[L] are ignored, as by any real inverse transform
-        float2 v[RD::RA];
+        float2 v[Q][RD::RA];
         if (t < L / RD::RA) {
 #pragma unroll
             for (int r = 0; r < RD::RA; ++r) {
                 const int k = t + r * (L / RD::RA);
-                float2 xk = B[k];
-                float2 xm = B[L - k];
-                if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
-                xm.y = -xm.y;
-                float2 s = cadd(xk, xm), d = csub(xk, xm);
-                float2 e = cmulc(d, __ldg(&a.tw[k]));
-                v[r] = make_float2(s.x - e.y, s.y + e.x);
+                const int km = L - k;
+                const float2 tk = __ldg(&a.tw[k]);
+                const int ik = (k / KB) * (R * KB) + (k % KB);
+                const int im = (km / KB) * (R * KB) + (km % KB);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const int rr = ry * Q + q;
+                    float2 xk = CB[ik + rr * KB];
+                    float2 xm = CB[im + rr * KB];
+                    if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
+                    xm.y = -xm.y;
+                    float2 s = cadd(xk, xm), d = csub(xk, xm);
+                    float2 e = cmulc(d, tk);
+                    v[q][r] = make_float2(s.x - e.y, s.y + e.x);
+                }
             }
         }
-        __syncthreads();  // the row buffer becomes the exchange tile
-        line_fft<RD, +1>(v, w, t, a.twL, smem);
+        __syncthreads();  // the staged rows become the exchange tiles
+        line_fft<RD, +1, Q, true>(v, w, t, a.twL, smem);
     }
+    if (!wait_all(&bars[1], 0, a.err, 3 << 8)) return;
 
     // ---- pointwise op on x[2n], x[2n+1], n = t + r*SL
-    if (t < SL && rvalid) {
-        const long long rbase = (long long) row * a.X;
-        const long long gbase = (long long) zz * a.N * a.GP + (long long) yy * a.GP;
+    if (t < SL) {
 #pragma unroll
-        for (int r = 0; r < RD::RL; ++r) {
-            const int c0 = 2 * (t + r * SL);
-            const bool img0 = in_img_row && c0 < a.M;
-            const bool img1 = in_img_row && c0 + 1 < a.M;
-            w[r] = x_op(a, op, rbase, gbase, c0, img0, img1, w[r].x, w[r].y, bg, acc);
+        for (int q = 0; q < Q; ++q) {
+            const int rr = ry * Q + q;
+            const int yy = y0 + rr;
+            if (yy < a.Y) {
+                const bool in_img_row = yy < a.N && z < a.P;
+                const long long rbase = ((long long) z * a.Y + yy) * XP;
+                const float *sx = (rg ? RB + rr * a.GP : RB + rr * XP);
+                const float *sxp = RB + C::REAL_F + rr * XP;
+                const float *sw = rw ? RB + 2 * C::REAL_F + rr * XP : nullptr;
+                x_row_op<FAM, RD::RL, SL>(a, op, t, rbase, sx, sxp, sw, in_img_row, bg, w[q], acc);
+            }
         }
     }
 
-    if (op == XOP_RATIO_SHB || op == XOP_RATIO_RL || op == XOP_ERROR_ONLY) {
-        // deterministic block reduction of the error partial (fixed order;
-        // the block may end in a partial warp, so lanes meet in shared memory)
-        double *red = reinterpret_cast<double *>(smx + (size_t) C::ROW_F2 * R);
-        const int tid = threadIdx.y * C::TPL + threadIdx.x;
+    if constexpr (rg) {
+        // deterministic reduction of the tile's error partial (fixed order;
+        // lanes meet in shared memory, then one full warp reduces)
         red[tid] = acc;
         __syncthreads();
         if (tid < 32) {
-            double s = 0.0;
-            for (int i = tid; i < C::THREADS; i += 32) s += red[i];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if (tid == 0) a.partial[blockIdx.x] = s;
+            double s2 = 0.0;
+            for (int i = tid; i < C::THREADS; i += 32) s2 += red[i];
+            for (int o = 16; o > 0; o >>= 1) s2 += __shfl_down_sync(0xffffffffu, s2, o);
+            if (tid == 0) a.partial[tile] = s2;
         }
     }
+    if constexpr (FAM == XFAM_STORE) return;
     if (!a.r2c) return;
 
     // ---- forward with the reversed radix list; w is its first-stage input
-    __syncthreads();  // all reads of the exchange tile are complete
-    float2 q[RV::RL];
-    line_fft<RV, -1>(w, q, t, a.twL, smem);
+    __syncthreads();  // all reads of the exchange tiles are complete
+    float2 qo[Q][RV::RL];
+    line_fft<RV, -1, Q, true>(w, qo, t, a.twL, smem);
     constexpr int SQ = L / RV::RL;
     __syncthreads();
     if (t < SQ) {
 #pragma unroll
-        for (int r = 0; r < RV::RL; ++r) B[t + r * SQ] = q[r];
+        for (int q = 0; q < Q; ++q)
+#pragma unroll
+            for (int r = 0; r < RV::RL; ++r) *smem(q, t + r * SQ) = qo[q][r];
     }
     __syncthreads();
-    // ---- Hermitian post-processing: X[k] = E[k] + W_X^k O[k], k = 0..L
-    if (rvalid) {
-        for (int k = t; k <= L; k += C::TPL) {
-            float2 zk = B[k == L ? 0 : k];
-            float2 zm = B[k == 0 ? 0 : L - k];
-            zm.y = -zm.y;
-            float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
-            float2 d = csub(zk, zm);
-            float2 o = make_float2(0.5f * d.y, -0.5f * d.x);  // -(i/2) d
-            Srow[k] = cadd(e, cmul(o, __ldg(&a.tw[k])));
-        }
+    // ---- Hermitian post-processing X[k] = E[k] + W_X^k O[k], k = 0..L,
+    // written to the blocked layout: thread e -> (kb, row, ki)
+    float2 *Sz = a.S + (long long) z * plane + (long long) y0 * KB;
+    for (int e = tid; e < C::NKB * R * KB; e += C::THREADS) {
+        const int ki = e % KB;
+        const int r2 = (e / KB) % R;
+        const int kb = e / (KB * R);
+        const int k = kb * KB + ki;
+        if (k > L || y0 + r2 >= a.Y) continue;
+        const float2 *Br = CB + (size_t) r2 * C::ROW_F2;
+        float2 zk = Br[k == L ? 0 : k];
+        float2 zm = Br[k == 0 ? 0 : L - k];
+        zm.y = -zm.y;
+        float2 ev = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+        float2 d = csub(zk, zm);
+        float2 o = make_float2(0.5f * d.y, -0.5f * d.x);  // -(i/2) d
+        Sz[(long long) kb * a.Y * KB + r2 * KB + ki] = cadd(ev, cmul(o, __ldg(&a.tw[k])));
     }
 }
 
