@@ -246,6 +246,8 @@ def main():
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    # with kernel timing on, the engine launches eagerly (events between
+    # kernels, no graph); the steps run back to back and are read at the end
     ev0.record(stream)
     for _ in range(args.steps):
         res = step()
@@ -258,6 +260,16 @@ def main():
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
+    # the same steps without per-kernel events (the loop as one cached CUDA graph)
+    torch.cuda.synchronize()
+    e2a = torch.cuda.Event(enable_timing=True)
+    e2b = torch.cuda.Event(enable_timing=True)
+    e2a.record(stream)
+    for _ in range(args.steps):
+        step()
+    e2b.record(stream)
+    torch.cuda.synchronize()
+    ms_noprof = e2a.elapsed_time(e2b)
     t_max = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
     if world > 1:
         dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
@@ -337,6 +349,10 @@ def main():
         "kernels": kernels[:8],
         "kernel_share": {k["name"]: round(k["ms"] / total_k, 3) for k in kernels[:8]},
         "iteration_ms": (ms_max / args.steps - res.seconds_setup * 1e3) / ITERS if res else None,
+        "diagnostics": {"ms_per_step_without_kernel_events": ms_noprof / args.steps,
+                        "setup_ms": res.seconds_setup * 1e3, "iterate_ms": res.seconds_iterate * 1e3,
+                        "host_enqueue_ms": res.seconds_enqueue * 1e3,
+                        "kernel_ms_per_step": total_k / args.steps},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -73,6 +73,7 @@ class Opts(ctypes.Structure):
         ("work", ctypes.c_int64 * 3),
         ("seconds_setup", ctypes.c_double),
         ("seconds_iterate", ctypes.c_double),
+        ("seconds_enqueue", ctypes.c_double),
     ]
 
 
@@ -203,6 +204,7 @@ class Result:
         self.work = tuple(o.work)
         self.seconds_setup = o.seconds_setup
         self.seconds_iterate = o.seconds_iterate
+        self.seconds_enqueue = o.seconds_enqueue
 
 
 def run_method(im: np.ndarray, psf: np.ndarray, **kw) -> Result:

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -67,6 +68,7 @@ static int fail(int code, const char *fmt, ...)
 struct ProfRec {
     int cls;
     cudaEvent_t a, b;
+    bool owned_by_graph;  // events live in a cached graph: never returned to the pool
 };
 struct ProfClass {
     std::string name;
@@ -112,6 +114,7 @@ struct ProfScope {
         rec.cls = prof_class(name, bytes);
         rec.a = prof_event();
         rec.b = prof_event();
+        rec.owned_by_graph = capturing(s);
         // inside stream capture a plain record is only a dependency edge;
         // the external flag makes it a timing node of the graph
         cudaEventRecordWithFlags(rec.a, st, capturing(st) ? cudaEventRecordExternal : 0);
@@ -230,6 +233,8 @@ static long long x_blocks(const Geometry &g) { return g.Z * ((g.Y + g.xp->R - 1)
 struct DeviceCtx {
     int device = -1;
     cudaStream_t stream = nullptr;
+    float *h_err = nullptr;  // pinned slot for per-iteration error readback (one per device)
+    std::mutex h_err_mu;
     std::map<long long, float2 *> tw;  // length -> exp(-2 pi i m / length)
 };
 
@@ -254,6 +259,7 @@ static int get_ctx(int device, DeviceCtx **out)
     auto *c = new DeviceCtx();
     c->device = device;
     CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CU(cudaMallocHost(&c->h_err, 64 * sizeof(float)));
     g_ctx[device] = c;
     *out = c;
     return DWCU_SUCCESS;
@@ -278,6 +284,105 @@ static int get_twiddles(DeviceCtx *c, long long n, const float2 **out)
     c->tw[n] = d;
     *out = d;
     return DWCU_SUCCESS;
+}
+
+// ------------------------------------------------------------ memory blocks
+//
+// A job's device memory is one block.  Released blocks are kept per device
+// (a few at most) and handed to the next job of the same size, so a stream of
+// equal-sized jobs (tiles, repeated deconvolutions) allocates once; the
+// iteration graphs captured on a block stay valid with it and are reused.
+
+struct Block {
+    char *ptr = nullptr;
+    size_t bytes = 0;
+    int device = 0;
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        long long kernels = 0;
+        std::vector<ProfRec> recs;  // timing events recorded by the graph's nodes
+    };
+    std::map<std::string, Graph> graphs;
+};
+
+static std::mutex g_blk_mu;
+static std::map<int, std::vector<Block *>> g_blk_free;
+constexpr size_t kMaxCachedBlocks = 2;
+
+static bool trace_on()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("DWCU_TRACE");
+        on = (e && *e && *e != '0') ? 1 : 0;
+    }
+    return on == 1;
+}
+
+static void block_free(Block *b)
+{
+    if (!b) return;
+    for (auto &kv : b->graphs) {
+        cudaGraphExecDestroy(kv.second.exec);
+        for (auto &r : kv.second.recs) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+    }
+    if (b->ptr) cudaFree(b->ptr);
+    delete b;
+}
+
+static Block *block_get(int device, size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_blk_mu);
+        auto &v = g_blk_free[device];
+        for (size_t i = 0; i < v.size(); ++i) {
+            if (v[i]->bytes == bytes) {
+                Block *b = v[i];
+                v.erase(v.begin() + (long) i);
+                return b;
+            }
+        }
+    }
+    Block *b = new Block();
+    b->bytes = bytes;
+    b->device = device;
+    cudaError_t e = cudaMalloc(&b->ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        // release the cached blocks of this device and retry once
+        std::vector<Block *> drop;
+        {
+            std::lock_guard<std::mutex> lk(g_blk_mu);
+            drop.swap(g_blk_free[device]);
+        }
+        for (auto *d : drop) block_free(d);
+        e = cudaMalloc(&b->ptr, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            delete b;
+            return nullptr;
+        }
+    }
+    return b;
+}
+
+static void block_put(Block *b)
+{
+    if (!b) return;
+    std::vector<Block *> drop;
+    {
+        std::lock_guard<std::mutex> lk(g_blk_mu);
+        auto &v = g_blk_free[b->device];
+        v.push_back(b);
+        while (v.size() > kMaxCachedBlocks) {
+            drop.push_back(v.front());
+            v.erase(v.begin());
+        }
+    }
+    for (auto *d : drop) block_free(d);
 }
 
 // ------------------------------------------------------------ host iterator
@@ -329,6 +434,7 @@ struct dwcu_job {
     dwcu::DeviceCtx *ctx = nullptr;
     cudaStream_t stream = nullptr;
     // device memory
+    dwcu::Block *block = nullptr;
     char *base = nullptr;
     size_t bytes = 0;
     float *gimg = nullptr;
@@ -351,11 +457,11 @@ struct dwcu_job {
     int done_iters = 0;
     bool finished = false;
     bool setup_done = false;
-    float *h_err = nullptr;        // pinned readback slot
     std::vector<float> trace;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     bool loop_started = false;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr; // a graph owned by this job (holding timing events)
+    double enqueue_s = 0;          // host time inside job_step
 };
 
 namespace dwcu {
@@ -560,13 +666,10 @@ static int alloc_job(dwcu_job *j)
     size_t o_ap = take(sizeof(ArgmaxPartial) * (size_t) j->n_apart);
     size_t o_psf = take(sizeof(float) * (size_t) npsf);
     j->bytes = off;
-    cudaError_t e = cudaMalloc(&j->base, off);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        j->base = nullptr;
-        return fail(DWCU_ERROR_OUT_OF_MEMORY, "cudaMalloc of %.3f GB for the job failed: %s", off / 1e9,
-                    cudaGetErrorString(e));
-    }
+    j->block = block_get(j->s.device, off);
+    if (!j->block)
+        return fail(DWCU_ERROR_OUT_OF_MEMORY, "cudaMalloc of %.3f GB for the job failed", off / 1e9);
+    j->base = j->block->ptr;
     char *b = j->base;
     j->gimg = (float *) (b + o_g);
     j->S = (float2 *) (b + o_S);
@@ -629,8 +732,6 @@ static int job_create(long long M, long long N, long long P, long long pM, long 
     if (rc == DWCU_SUCCESS) rc = get_twiddles(ctx, g.X / 2, &j->tw_l);
     if (rc == DWCU_SUCCESS && g.Y > 1) rc = get_twiddles(ctx, g.Y, &j->tw_y);
     if (rc == DWCU_SUCCESS) rc = get_twiddles(ctx, g.Z, &j->tw_z);
-    if (rc == DWCU_SUCCESS && cudaMallocHost(&j->h_err, sizeof(float)) != cudaSuccess)
-        rc = fail(DWCU_ERROR_OUT_OF_MEMORY, "pinned allocation failed");
     if (rc == DWCU_SUCCESS &&
         (cudaEventCreate(&j->ev0) != cudaSuccess || cudaEventCreate(&j->ev1) != cudaSuccess ||
          cudaEventCreate(&j->ev2) != cudaSuccess))
@@ -730,7 +831,16 @@ static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_dev
 // Enqueue iterations.  FIXED: no host synchronisation (and, if requested, the
 // whole remaining loop as one CUDA graph).  REL/ABS: each error is read back
 // before deciding whether the next iteration runs (dw.c:237-270).
+static int job_step_impl(dwcu_job *j, int nmax, int *remaining);
 static int job_step(dwcu_job *j, int nmax, int *remaining)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = job_step_impl(j, nmax, remaining);
+    j->enqueue_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+static int job_step_impl(dwcu_job *j, int nmax, int *remaining)
 {
     if (!j->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "job_step before job_setup");
     CU(cudaSetDevice(j->s.device));
@@ -749,25 +859,89 @@ static int job_step(dwcu_job *j, int nmax, int *remaining)
     while (!j->finished && ran < nmax) {
         const int k = j->k_next;
         if (fixed) {
-            const bool use_graph = j->s.use_graph && nmax >= (j->it.niter - k) && (j->it.niter - k) > 1 && !j->graph;
+            bool prof_now;
+            {
+                std::lock_guard<std::mutex> lk(g_prof_mu);
+                prof_now = g_prof_on;
+            }
+            // with kernel timing on, launches stay eager: timing events inside
+            // a graph make every replay expensive on the host
+            const bool use_graph = j->s.use_graph && !prof_now && nmax >= (j->it.niter - k) && (j->it.niter - k) > 1;
             if (use_graph) {
-                // capture the whole remaining loop into one graph
-                cudaGraph_t gr = nullptr;
-                CU(cudaStreamBeginCapture(j->stream, cudaStreamCaptureModeThreadLocal));
-                int rc = DWCU_SUCCESS;
-                for (int kk = k; kk < j->it.niter && rc == DWCU_SUCCESS; ++kk) rc = run_one_fixed(kk);
-                cudaError_t ce = cudaStreamEndCapture(j->stream, &gr);
-                if (rc != DWCU_SUCCESS) {
-                    if (gr) cudaGraphDestroy(gr);
-                    return rc;
+                // The whole remaining loop as one graph.  A graph captured
+                // earlier on this memory block for the same sizes, options
+                // and starting state is launched again (its kernels carry
+                // the same pointers and parameters).
+                bool prof;
+                {
+                    std::lock_guard<std::mutex> lk(g_prof_mu);
+                    prof = g_prof_on;
                 }
-                if (ce != cudaSuccess) return fail(DWCU_ERROR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+                char key[512];
+                const Geometry &gg = j->g;
+                snprintf(key, sizeof key,
+                         "%lld %lld %lld %lld %lld %lld %lld %lld %lld|%d %d %d %d %d %d %d %a|%d %d %d %p %p",
+                         gg.M, gg.N, gg.P, gg.pM, gg.pN, gg.pP, gg.X, gg.Y, gg.Z, j->s.method, j->it.niter,
+                         j->s.maxiter, k, j->s.metric, j->s.positivity, j->s.border_quality, (double) j->s.alphamax,
+                         (int) j->spectrum_ready, (int) (j->W != nullptr), (int) prof, (void *) j->xa, (void *) j->xb);
+                const std::string skey(key);
                 cudaGraphExec_t ex = nullptr;
-                ce = cudaGraphInstantiate(&ex, gr, 0);
-                cudaGraphDestroy(gr);
-                if (ce != cudaSuccess) return fail(DWCU_ERROR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
-                CU(cudaGraphLaunch(ex, j->stream));  // its kernels were counted at capture
-                j->graph = ex;
+                auto hit = j->block->graphs.find(skey);
+                long long kernels = 0;
+                if (hit != j->block->graphs.end()) {
+                    ex = hit->second.exec;
+                    // the buffer roles the loop leaves behind (SHB swaps after
+                    // every update; the last iteration has none)
+                    if (shb)
+                        for (int kk = k; kk < j->it.niter - 1; ++kk) std::swap(j->xa, j->xb);
+                    g_launches += hit->second.kernels;
+                    if (prof) {
+                        // this replay re-records the graph's timing events
+                        std::lock_guard<std::mutex> lk(g_prof_mu);
+                        for (auto &r : hit->second.recs) g_prof_recs.push_back(r);
+                    }
+                } else {
+                    auto t0 = std::chrono::steady_clock::now();
+                    cudaGraph_t gr = nullptr;
+                    CU(cudaStreamBeginCapture(j->stream, cudaStreamCaptureModeThreadLocal));
+                    int rc = DWCU_SUCCESS;
+                    const long long l0 = g_launches;
+                    size_t r0;
+                    {
+                        std::lock_guard<std::mutex> lk(g_prof_mu);
+                        r0 = g_prof_recs.size();
+                    }
+                    for (int kk = k; kk < j->it.niter && rc == DWCU_SUCCESS; ++kk) rc = run_one_fixed(kk);
+                    kernels = g_launches - l0;
+                    std::vector<ProfRec> grecs;
+                    {
+                        std::lock_guard<std::mutex> lk(g_prof_mu);
+                        if (g_prof_recs.size() > r0) grecs.assign(g_prof_recs.begin() + (long) r0, g_prof_recs.end());
+                    }
+                    cudaError_t ce = cudaStreamEndCapture(j->stream, &gr);
+                    if (rc != DWCU_SUCCESS) {
+                        if (gr) cudaGraphDestroy(gr);
+                        return rc;
+                    }
+                    if (ce != cudaSuccess)
+                        return fail(DWCU_ERROR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+                    auto t1 = std::chrono::steady_clock::now();
+                    ce = cudaGraphInstantiate(&ex, gr, 0);
+                    cudaGraphDestroy(gr);
+                    if (ce != cudaSuccess)
+                        return fail(DWCU_ERROR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+                    auto t2 = std::chrono::steady_clock::now();
+                    if (trace_on())
+                        fprintf(stderr, "dwcu: captured %lld kernels in %.1f ms, instantiated in %.1f ms\n", kernels,
+                                std::chrono::duration<double, std::milli>(t1 - t0).count(),
+                                std::chrono::duration<double, std::milli>(t2 - t1).count());
+                    Block::Graph gent;
+                    gent.exec = ex;
+                    gent.kernels = kernels;
+                    gent.recs = grecs;
+                    j->block->graphs[skey] = gent;
+                }
+                CU(cudaGraphLaunch(ex, j->stream));  // its kernels are counted at capture (or replayed above)
                 ran += j->it.niter - k;
                 j->done_iters = j->it.niter;
                 j->it.iter = j->it.niter;
@@ -786,9 +960,13 @@ static int job_step(dwcu_job *j, int nmax, int *remaining)
         // REL / ABS: forward half, read the error, decide
         if (!j->spectrum_ready) TRY(iter_input(j, k));
         TRY(iter_forward(j, k, true));
-        CU(cudaMemcpyAsync(j->h_err, j->err + k, sizeof(float), cudaMemcpyDeviceToHost, j->stream));
-        CU(cudaStreamSynchronize(j->stream));
-        const float e = *j->h_err;
+        float e;
+        {
+            std::lock_guard<std::mutex> lk(j->ctx->h_err_mu);
+            CU(cudaMemcpyAsync(j->ctx->h_err, j->err + k, sizeof(float), cudaMemcpyDeviceToHost, j->stream));
+            CU(cudaStreamSynchronize(j->stream));
+            e = *j->ctx->h_err;
+        }
         j->it.set(e);
         j->trace[(size_t) k] = e;
         j->done_iters = k + 1;
@@ -851,6 +1029,7 @@ static int job_result(dwcu_job *j, float *out, bool on_device, dwcu_opts *so)
         cudaEventElapsedTime(&ms_loop, j->ev1, j->ev2);
         so->seconds_setup = ms_setup * 1e-3;
         so->seconds_iterate = ms_loop * 1e-3;
+        so->seconds_enqueue = j->enqueue_s;
         if (so->error_trace)
             for (int i = 0; i < nerr && i < so->trace_capacity; ++i) so->error_trace[i] = errs[(size_t) i];
         if (j->s.verbosity > 0 && j->s.iter_type == DWCU_ITER_FIXED)
@@ -1065,8 +1244,7 @@ void dwcu_job_destroy(dwcu_job *j)
     cudaSetDevice(j->s.device);
     if (j->stream) cudaStreamSynchronize(j->stream);
     if (j->graph) cudaGraphExecDestroy(j->graph);
-    if (j->base) cudaFree(j->base);
-    if (j->h_err) cudaFreeHost(j->h_err);
+    if (j->block) block_put(j->block);
     if (j->ev0) cudaEventDestroy(j->ev0);
     if (j->ev1) cudaEventDestroy(j->ev1);
     if (j->ev2) cudaEventDestroy(j->ev2);
@@ -1119,8 +1297,10 @@ int dwcu_profile_collect(dwcu_kernel_stat *stats, int32_t capacity, int32_t *cou
         } else {
             cudaGetLastError();
         }
-        g_prof_pool.push_back(r.a);
-        g_prof_pool.push_back(r.b);
+        if (!r.owned_by_graph) {
+            g_prof_pool.push_back(r.a);
+            g_prof_pool.push_back(r.b);
+        }
     }
     g_prof_recs.clear();
     int k = 0;

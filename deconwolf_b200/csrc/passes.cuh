@@ -49,16 +49,19 @@ struct Rad {
     static __device__ __forceinline__ int pad(int idx) { return idx + idx / RA; }
 };
 
-// Twiddles of one Stockham stage for butterfly index j: W_{NS*R}^{r*(j mod NS)},
-// r = 1 .. R-1, loaded from the length-N table.  They depend only on j, so a
-// stage's twiddles are loaded before the barrier that precedes the stage.
+// Twiddles of one Stockham stage for butterfly index j: W^r with
+// W = W_{NS*R}^{j mod NS}, r = 1 .. R-1.  One value comes from the length-N
+// table; the other powers are products of it (squarings for even r), at most
+// six products deep, so the twiddles cost one load per stage instead of R-1
+// (with most of shared memory in use, the table does not stay in L1).
 template <int N, int NS, int R>
 __device__ __forceinline__ void stage_twiddles(float2 (&w)[R], int j, const float2 *__restrict__ tw)
 {
     constexpr int step = N / (NS * R);
     const int u = (j % NS) * step;
+    if constexpr (R > 1) w[1] = __ldg(&tw[u]);
 #pragma unroll
-    for (int r = 1; r < R; ++r) w[r] = __ldg(&tw[r * u]);
+    for (int r = 2; r < R; ++r) w[r] = (r % 2 == 0) ? cmul(w[r / 2], w[r / 2]) : cmul(w[r - 1], w[1]);
 }
 
 // one Stockham butterfly on Q rows that share the butterfly index:
@@ -444,6 +447,16 @@ __host__ __device__ constexpr int x_family(int op)
 }
 
 __device__ __forceinline__ bool op_c2r(int op) { return op >= XOP_RATIO_SHB; }
+
+// err_term with the quotient g/y already computed (q is only read when
+// y > 0 and g > 0, where it equals g/y)
+__device__ __forceinline__ double err_term_q(float yv, float gv, float q, int metric)
+{
+    const double y = yv, g = gv;
+    if (metric == 0) return (y - g) * (y - g);
+    if (yv > 0.f && gv > 0.f) return g * (double) logf(q) - (g - y);
+    return 0.0;
+}
 __device__ __forceinline__ bool op_reads_x(int op)
 {
     return op == XOP_FWD_COPY || op == XOP_FWD_SHBP || op == XOP_UPDATE_SHB || op == XOP_UPDATE_RL;
@@ -503,8 +516,6 @@ __device__ __forceinline__ void x_row_op(const XArgs &a, int op, int t, long lon
             const float y0 = w[r].x, y1 = w[r].y;
             const float g0 = img0 ? sx[c0] : 0.f;
             const float g1 = img1 ? sx[c0 + 1] : 0.f;
-            if (img0) acc += err_term(y0, g0, a.metric);
-            if (img1) acc += err_term(y1, g1, a.metric);
             float v0 = 0.f, v1 = 0.f;
             if (op == XOP_RATIO_SHB) {
                 // method_shb.c:31-48: |y| < 1e-6 -> +-1e-6; r = g/y on the image, 0 elsewhere
@@ -513,10 +524,18 @@ __device__ __forceinline__ void x_row_op(const XArgs &a, int op, int t, long lon
                 if ((double) fabsf(d1) < 1e-6) d1 = copysignf(1e-6f, d1);
                 v0 = img0 ? g0 / d0 : 0.f;
                 v1 = img1 ? g1 / d1 : 0.f;
+                // the error's g/y is the same quotient unless the guard changed y
+                if (img0) acc += err_term_q(y0, g0, d0 == y0 ? v0 : g0 / y0, a.metric);
+                if (img1) acc += err_term_q(y1, g1, d1 == y1 ? v1 : g1 / y1, a.metric);
             } else if (op == XOP_RATIO_RL) {
                 // method_rl.c:46-67: r = g/y if y > 0 else bg on the image, 1e-6 elsewhere
                 v0 = img0 ? (y0 > 0.f ? g0 / y0 : bg) : 1e-6f;
                 v1 = img1 ? (y1 > 0.f ? g1 / y1 : bg) : 1e-6f;
+                if (img0) acc += err_term_q(y0, g0, v0, a.metric);  // used only when y > 0
+                if (img1) acc += err_term_q(y1, g1, v1, a.metric);
+            } else {
+                if (img0) acc += err_term_q(y0, g0, y0 > 0.f ? g0 / y0 : 0.f, a.metric);
+                if (img1) acc += err_term_q(y1, g1, y1 > 0.f ? g1 / y1 : 0.f, a.metric);
             }
             w[r] = make_float2(v0, v1);
         }

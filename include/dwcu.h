@@ -78,6 +78,7 @@ typedef struct dwcu_opts {
     int64_t work[3];         /* padded job size used (X, Y, Z) */
     double seconds_setup;    /* device time before the first iteration */
     double seconds_iterate;  /* device time of the iteration loop */
+    double seconds_enqueue;  /* host time spent issuing the iterations (graph capture included) */
 } dwcu_opts;
 
 /* Defaults of dw_opts_new (src/dw.c:340-413) for the fields above. */
