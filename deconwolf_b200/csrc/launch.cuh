@@ -78,7 +78,7 @@ template <class RD, int R, int FAM>
 void launch_x_fam(const XArgs &a, cudaStream_t st)
 {
     static KernelOnce ko;
-    using C = XCfg<RD, R>;
+    using C = XCfg<RD, R, FAM>;
     ensure_smem(ko, k_xpass<RD, R, FAM>, C::SMEM_BYTES);
     k_xpass<RD, R, FAM><<<a.ntiles, dim3(C::TPL, C::RY), C::SMEM_BYTES, st>>>(a);
 }

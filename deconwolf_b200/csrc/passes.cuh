@@ -392,7 +392,11 @@ struct XArgs {
 // and, on a second barrier, of its real rows; the real rows arrive while the
 // inverse transform runs.  Three CTAs share an SM, so one CTA's copies
 // overlap the others' arithmetic.
-template <class RD, int R>
+// real slots a family stages: forward: x, x_{k-1}; ratio: the image rows;
+// update: x, x_{k-1}, W; C2R-store: none
+__host__ __device__ constexpr int x_slots(int fam) { return fam == 0 ? 2 : fam == 1 ? 1 : fam == 2 ? 3 : 0; }
+
+template <class RD, int R, int FAM = 2>
 struct XCfg {
     using RV = RevRad<RD>;
     static constexpr int Q = 1;                     // rows per thread
@@ -411,9 +415,11 @@ struct XCfg {
     // complex area and three real slots: x (or the image rows g, which no op
     // reads together with x), xp, W
     static constexpr size_t REAL_OFF = 64 + sizeof(float2) * (size_t) AREA_F2;
-    static constexpr size_t RED_OFF = REAL_OFF + 3 * sizeof(float) * (size_t) REAL_F;
+    static constexpr size_t RED_OFF = REAL_OFF + x_slots(FAM) * sizeof(float) * (size_t) REAL_F;
     static constexpr size_t SMEM_BYTES = RED_OFF + sizeof(double) * THREADS;
-    static constexpr int MIN_BLOCKS = (SMEM_BYTES * 3 <= 225 * 1024 && THREADS * 3 <= 2048) ? 3 : 1;
+    // resident CTAs per SM to aim for (registers are capped to fit them)
+    static constexpr int MIN_BLOCKS = (SMEM_BYTES * 4 <= 224 * 1024 && THREADS * 4 <= 2048) ? 4
+                                    : (SMEM_BYTES * 3 <= 225 * 1024 && THREADS * 3 <= 2048) ? 3 : 1;
     static_assert(R % Q == 0, "rows per tile");
     static_assert(THREADS >= 32, "the error reduction needs one full warp");
 };
@@ -505,7 +511,45 @@ __device__ __forceinline__ void x_row_op(const XArgs &a, int op, int t, long lon
         }
         break;
     case XOP_RATIO_SHB:
+        if constexpr (FAM != XFAM_RATIO) break;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const int c0 = 2 * (t + r * SL);
+            const bool img0 = in_img_row && c0 < M;
+            const bool img1 = in_img_row && c0 + 1 < M;
+            const float y0 = w[r].x, y1 = w[r].y;
+            const float g0 = img0 ? sx[c0] : 0.f;
+            const float g1 = img1 ? sx[c0 + 1] : 0.f;
+            // method_shb.c:31-48: |y| < 1e-6 -> +-1e-6; r = g/y on the image, 0 elsewhere.
+            // (double)|y| < 1e-6 holds exactly when |y| <= 1e-6f, the float just below 1e-6.
+            const float d0 = fabsf(y0) <= 1e-6f ? copysignf(1e-6f, y0) : y0;
+            const float d1 = fabsf(y1) <= 1e-6f ? copysignf(1e-6f, y1) : y1;
+            const float v0 = img0 ? g0 / d0 : 0.f;
+            const float v1 = img1 ? g1 / d1 : 0.f;
+            // the error's g/y is the same quotient unless the guard changed y
+            if (img0) acc += err_term_q(y0, g0, d0 == y0 ? v0 : g0 / y0, a.metric);
+            if (img1) acc += err_term_q(y1, g1, d1 == y1 ? v1 : g1 / y1, a.metric);
+            w[r] = make_float2(v0, v1);
+        }
+        break;
     case XOP_RATIO_RL:
+        if constexpr (FAM != XFAM_RATIO) break;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+            const int c0 = 2 * (t + r * SL);
+            const bool img0 = in_img_row && c0 < M;
+            const bool img1 = in_img_row && c0 + 1 < M;
+            const float y0 = w[r].x, y1 = w[r].y;
+            const float g0 = img0 ? sx[c0] : 0.f;
+            const float g1 = img1 ? sx[c0 + 1] : 0.f;
+            // method_rl.c:46-67: r = g/y if y > 0 else bg on the image, 1e-6 elsewhere
+            const float v0 = img0 ? (y0 > 0.f ? g0 / y0 : bg) : 1e-6f;
+            const float v1 = img1 ? (y1 > 0.f ? g1 / y1 : bg) : 1e-6f;
+            if (img0) acc += err_term_q(y0, g0, v0, a.metric);  // q used only when y > 0
+            if (img1) acc += err_term_q(y1, g1, v1, a.metric);
+            w[r] = make_float2(v0, v1);
+        }
+        break;
     case XOP_ERROR_ONLY:
         if constexpr (FAM != XFAM_RATIO) break;
 #pragma unroll
@@ -516,28 +560,8 @@ __device__ __forceinline__ void x_row_op(const XArgs &a, int op, int t, long lon
             const float y0 = w[r].x, y1 = w[r].y;
             const float g0 = img0 ? sx[c0] : 0.f;
             const float g1 = img1 ? sx[c0 + 1] : 0.f;
-            float v0 = 0.f, v1 = 0.f;
-            if (op == XOP_RATIO_SHB) {
-                // method_shb.c:31-48: |y| < 1e-6 -> +-1e-6; r = g/y on the image, 0 elsewhere
-                float d0 = y0, d1 = y1;
-                if ((double) fabsf(d0) < 1e-6) d0 = copysignf(1e-6f, d0);
-                if ((double) fabsf(d1) < 1e-6) d1 = copysignf(1e-6f, d1);
-                v0 = img0 ? g0 / d0 : 0.f;
-                v1 = img1 ? g1 / d1 : 0.f;
-                // the error's g/y is the same quotient unless the guard changed y
-                if (img0) acc += err_term_q(y0, g0, d0 == y0 ? v0 : g0 / y0, a.metric);
-                if (img1) acc += err_term_q(y1, g1, d1 == y1 ? v1 : g1 / y1, a.metric);
-            } else if (op == XOP_RATIO_RL) {
-                // method_rl.c:46-67: r = g/y if y > 0 else bg on the image, 1e-6 elsewhere
-                v0 = img0 ? (y0 > 0.f ? g0 / y0 : bg) : 1e-6f;
-                v1 = img1 ? (y1 > 0.f ? g1 / y1 : bg) : 1e-6f;
-                if (img0) acc += err_term_q(y0, g0, v0, a.metric);  // used only when y > 0
-                if (img1) acc += err_term_q(y1, g1, v1, a.metric);
-            } else {
-                if (img0) acc += err_term_q(y0, g0, y0 > 0.f ? g0 / y0 : 0.f, a.metric);
-                if (img1) acc += err_term_q(y1, g1, y1 > 0.f ? g1 / y1 : 0.f, a.metric);
-            }
-            w[r] = make_float2(v0, v1);
+            if (img0) acc += err_term_q(y0, g0, y0 > 0.f ? g0 / y0 : 0.f, a.metric);
+            if (img1) acc += err_term_q(y1, g1, y1 > 0.f ? g1 / y1 : 0.f, a.metric);
         }
         break;
     case XOP_UPDATE_SHB:
@@ -615,10 +639,10 @@ __device__ __forceinline__ void x_row_op(const XArgs &a, int op, int t, long lon
 }
 
 template <class RD, int R, int FAM>
-__global__ void __launch_bounds__(XCfg<RD, R>::THREADS, XCfg<RD, R>::MIN_BLOCKS)
+__global__ void __launch_bounds__(XCfg<RD, R, FAM>::THREADS, XCfg<RD, R, FAM>::MIN_BLOCKS)
 k_xpass(XArgs a)
 {
-    using C = XCfg<RD, R>;
+    using C = XCfg<RD, R, FAM>;
     using RV = typename C::RV;
     constexpr int L = C::L;
     constexpr int Q = C::Q;
