@@ -99,13 +99,20 @@ def profile_collect() -> list[dict]:
                  bytes_per_launch=float(arr[i].bytes_per_launch)) for i in range(min(n.value, cap))]
 
 
+class Tile(ctypes.Structure):
+    """dwcu_tile: struct tile of src/tiling.h:29-34 (x, y, z order)."""
+    _fields_ = [("size", ctypes.c_int64 * 3), ("pos", ctypes.c_int64 * 6),
+                ("xpos", ctypes.c_int64 * 6), ("xsize", ctypes.c_int64 * 3)]
+
+
 # every symbol include/dwcu.h declares
 EXPORTS = [
     "dwcu_opts_init", "dwcu_deconvolve", "dwcu_deconvolve_device", "dwcu_plan_size",
     "dwcu_job_create", "dwcu_job_setup", "dwcu_job_step", "dwcu_job_done", "dwcu_job_result",
     "dwcu_job_destroy", "dwcu_job_set_stream", "dwcu_job_bytes", "dwcu_last_error",
     "dwcu_abi_version", "dwcu_device_count", "dwcu_launch_count", "dwcu_fft_r2c", "dwcu_fft_c2r",
-    "dwcu_profile_enable", "dwcu_profile_collect",
+    "dwcu_profile_enable", "dwcu_profile_collect", "dwcu_batch_run", "dwcu_psf_prepare",
+    "dwcu_tiling_create", "dwcu_deconvolve_tiled",
 ]
 
 _lib = None
@@ -158,6 +165,16 @@ def lib() -> ctypes.CDLL:
     for fn in (L.dwcu_fft_r2c, L.dwcu_fft_c2r):
         fn.argtypes = [vp, i64, i64, i64, vp, i32, vp]
         fn.restype = ctypes.c_int
+    L.dwcu_batch_run.argtypes = [ctypes.POINTER(vp), i32, vp]
+    L.dwcu_batch_run.restype = ctypes.c_int
+    L.dwcu_psf_prepare.argtypes = [vp, i64, i64, i64, i64, i64, i64, i32, ctypes.c_float, vp,
+                                   ctypes.POINTER(i64)]
+    L.dwcu_psf_prepare.restype = ctypes.c_int
+    L.dwcu_tiling_create.argtypes = [i64, i64, i64, i64, i64, ctypes.POINTER(Tile), i32, ctypes.POINTER(i32)]
+    L.dwcu_tiling_create.restype = ctypes.c_int
+    L.dwcu_deconvolve_tiled.argtypes = [vp, i64, i64, i64, vp, i64, i64, i64, i64, i64, ctypes.c_float,
+                                        ctypes.c_float, ctypes.c_double, P_opts, vp]
+    L.dwcu_deconvolve_tiled.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -267,6 +284,70 @@ def plan_size(shape, psf_shape, border_quality: int = 2, method: str = "shb"):
     return tuple(work), nbytes.value
 
 
+def psf_prepare(psf: np.ndarray, shape, border_quality: int = 2, xycropfactor: float = 0.001) -> np.ndarray:
+    """dw_run's PSF preparation for an image of ``shape`` (P, N, M): normalise,
+    psf_autocrop (dw.c:1973-1997), normalise (dwcu_psf_prepare)."""
+    p = np.ascontiguousarray(psf, dtype=np.float32)
+    P, N, M = shape
+    pP, pN, pM = p.shape
+    out = np.empty(p.size, dtype=np.float32)
+    dims = (ctypes.c_int64 * 3)()
+    _check(lib().dwcu_psf_prepare(p.ctypes.data, pM, pN, pP, M, N, P, border_quality, xycropfactor,
+                                  out.ctypes.data, dims))
+    return out[: dims[0] * dims[1] * dims[2]].reshape(dims[2], dims[1], dims[0]).copy()
+
+
+def tiling_create(shape, max_size: int, overlap: int = 20) -> list[dict]:
+    """tiling_create (tiling.c:70-130) for an image of ``shape`` (P, N, M);
+    each tile as a dict of x, y, z ordered ``size``, ``pos``, ``xpos``, ``xsize``."""
+    P, N, M = shape
+    n = ctypes.c_int32()
+    _check(lib().dwcu_tiling_create(M, N, P, max_size, overlap, None, 0, ctypes.byref(n)))
+    arr = (Tile * n.value)()
+    _check(lib().dwcu_tiling_create(M, N, P, max_size, overlap, arr, n.value, ctypes.byref(n)))
+    return [{k: tuple(getattr(t, k)) for k in ("size", "pos", "xpos", "xsize")} for t in arr]
+
+
+def deconvolve_tiled(im: np.ndarray, psf: np.ndarray, tile_size: int, overlap: int = 20,
+                     offset: float = 5.0, xycropfactor: float = 0.001, hbm_budget: float = 0.0,
+                     **kw) -> Result:
+    """deconvolve_tiles (dw.c:2001-2229) on host arrays; ``psf`` as dw_run
+    hands it over (already prepared for the whole image)."""
+    im = np.ascontiguousarray(im, dtype=np.float32)
+    psf = np.ascontiguousarray(psf, dtype=np.float32)
+    o = make_opts(**kw)
+    out = np.empty_like(im)
+    P, N, M = im.shape
+    pP, pN, pM = psf.shape
+    _check(lib().dwcu_deconvolve_tiled(im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP, tile_size,
+                                       overlap, offset, xycropfactor, hbm_budget, ctypes.byref(o),
+                                       out.ctypes.data))
+    return Result(out, np.zeros(0, np.float32), o)
+
+
+def batch_run(jobs: list["Job"], stream: int = 0) -> None:
+    """Run set-up jobs to completion together (dwcu_batch_run)."""
+    arr = (ctypes.c_void_p * len(jobs))(*[j.h.value for j in jobs])
+    _check(lib().dwcu_batch_run(arr, len(jobs), ctypes.c_void_p(stream or None)))
+
+
+def dw_run(image: np.ndarray, psf: np.ndarray, *, tilesize: int = 0, tilepad: int = 20,
+           offset: float = 5.0, xycropfactor: float = 0.001, **kw) -> np.ndarray:
+    """The method part of dw_run (dw.c:2797-2850) on in-memory arrays: PSF
+    normalised and cropped against the image, then the method on the whole
+    image (+offset; the returned buffer keeps the offset, as dw_run's result
+    buffer does, dw.c:2835-2848 and 2907-2913) or, with ``tilesize`` > 0,
+    deconvolve_tiles (offset removed per tile).  Options as :func:`make_opts`."""
+    im = np.array(image, dtype=np.float32, copy=True)
+    bq = kw.get("border_quality", 2)
+    p = psf_prepare(psf, im.shape, bq, xycropfactor)
+    if tilesize > 0:
+        return deconvolve_tiled(im, p, tilesize, tilepad, offset, xycropfactor, **kw).out
+    if offset > 0:
+        im += np.float32(offset)
+    return run_method(im, p, **kw).out
+
+
 class Job:
     """A resident deconvolution job (dwcu_job_*): setup once, step, read."""
 
@@ -332,8 +413,9 @@ def deconvolve(image: np.ndarray, psf: np.ndarray, iterations: int, bq: int = 2,
                threads: int | None = None, gpu: bool = True, *, method: str = "shb",
                offset: float = 5.0, device: int = 0) -> np.ndarray:
     """pydeconwolf.deconvolve(image, psf, iterations, bq, verbose, threads,
-    gpu) (pydeconwolf.c:284-394): fixed iteration count, PSF normalised to
-    sum 1 (dw.c:2799), offset added before the method (dw.c:2835-2838).
+    gpu) (pydeconwolf.c:284-394), which runs dw_run: fixed iteration count,
+    PSF prepared as in :func:`dw_run`, offset added before the method and
+    kept in the result (dw.c:2835-2848).
     ``threads`` is accepted for signature compatibility (the work runs on
     the GPU); ``gpu=False`` is rejected: this package has no CPU path."""
     if not gpu:
@@ -343,10 +425,5 @@ def deconvolve(image: np.ndarray, psf: np.ndarray, iterations: int, bq: int = 2,
         raise ValueError("The image contains negative values, can not continue!")  # dw.c:2703-2710
     if np.max(im) < 1.0:
         raise ValueError("The image has too low intensity, can not continue!")  # dw.c:2711-2721
-    p = np.array(psf, dtype=np.float32, copy=True)
-    p /= np.float32(p.sum(dtype=np.float64))
-    if offset > 0:
-        im += np.float32(offset)
-    res = run_method(im, p, method=method, n_iter=iterations, iter_type=ITER_FIXED,
-                     border_quality=bq, verbosity=verbose, device=device)
-    return res.out
+    return dw_run(im, psf, offset=offset, method=method, n_iter=iterations, iter_type=ITER_FIXED,
+                  border_quality=bq, verbosity=verbose, device=device)

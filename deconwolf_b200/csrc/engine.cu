@@ -46,6 +46,10 @@ static int fail(int code, const char *fmt, ...)
     return code;
 }
 
+// for the library's other translation units (host.cu)
+void record_error(const char *msg) { g_last_error = msg; }
+void record_launch() { ++g_launches; }
+
 #define CU(call)                                                                              \
     do {                                                                                      \
         cudaError_t e_ = (call);                                                              \
@@ -1040,6 +1044,108 @@ static int job_result(dwcu_job *j, float *out, bool on_device, dwcu_opts *so)
     return DWCU_SUCCESS;
 }
 
+// Run a batch of set-up jobs to completion together.  Jobs with a fixed
+// iteration count are captured into one CUDA graph with one stream per job:
+// the graph holds independent chains, so small jobs (tiles, channels) share
+// the GPU instead of running one after another.  Jobs with a REL/ABS stopping
+// rule are stepped round-robin, one iteration each, on their own streams.
+static int batch_run(dwcu_job **jobs, int n, cudaStream_t origin)
+{
+    if (n <= 0) return DWCU_SUCCESS;
+    const int dev = jobs[0]->s.device;
+    for (int i = 0; i < n; ++i) {
+        if (!jobs[i] || !jobs[i]->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "batch: job %d not set up", i);
+        if (jobs[i]->s.device != dev) return fail(DWCU_ERROR_INVALID_VALUE, "batch: jobs on different devices");
+    }
+    CU(cudaSetDevice(dev));
+    DeviceCtx *ctx = jobs[0]->ctx;
+    if (!origin) origin = ctx->stream;
+    // one stream per job (kept by the caller's jobs for the duration)
+    std::vector<cudaStream_t> streams((size_t) n);
+    std::vector<cudaStream_t> saved((size_t) n);
+    for (int i = 0; i < n; ++i) {
+        CU(cudaStreamCreateWithFlags(&streams[(size_t) i], cudaStreamNonBlocking));
+        saved[(size_t) i] = jobs[i]->stream;
+        jobs[i]->stream = streams[(size_t) i];
+    }
+    int rc = DWCU_SUCCESS;
+    std::vector<int> fixed_idx, rel_idx;
+    for (int i = 0; i < n; ++i) {
+        if (jobs[i]->finished) continue;
+        (jobs[i]->s.iter_type == DWCU_ITER_FIXED ? fixed_idx : rel_idx).push_back(i);
+    }
+    // prior work of every job (its setup) must finish before its chain runs
+    cudaEvent_t fork = nullptr, done = nullptr;
+    CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    for (int i = 0; i < n; ++i) {
+        cudaEvent_t e = nullptr;
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        cudaEventRecord(e, saved[(size_t) i]);
+        cudaStreamWaitEvent(origin, e, 0);
+        cudaEventDestroy(e);
+    }
+    if (!fixed_idx.empty()) {
+        bool prof;
+        {
+            std::lock_guard<std::mutex> lk(g_prof_mu);
+            prof = g_prof_on;
+        }
+        const bool graph = !prof;
+        cudaGraph_t gr = nullptr;
+        if (graph) CU(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal));
+        cudaEventRecord(fork, origin);
+        for (int i : fixed_idx) {
+            dwcu_job *j = jobs[i];
+            cudaStreamWaitEvent(j->stream, fork, 0);
+            const int ug = j->s.use_graph;
+            j->s.use_graph = 0;  // eager launches: captured into the batch graph
+            if (rc == DWCU_SUCCESS) rc = job_step_impl(j, 1 << 30, nullptr);
+            j->s.use_graph = ug;
+            cudaEventRecord(done, j->stream);
+            cudaStreamWaitEvent(origin, done, 0);
+        }
+        if (graph) {
+            cudaError_t ce = cudaStreamEndCapture(origin, &gr);
+            if (rc == DWCU_SUCCESS && ce != cudaSuccess)
+                rc = fail(DWCU_ERROR_CUDA, "batch capture failed: %s", cudaGetErrorString(ce));
+            cudaGraphExec_t ex = nullptr;
+            if (rc == DWCU_SUCCESS) {
+                ce = cudaGraphInstantiate(&ex, gr, 0);
+                if (ce != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "batch instantiate failed: %s", cudaGetErrorString(ce));
+            }
+            if (gr) cudaGraphDestroy(gr);
+            if (rc == DWCU_SUCCESS) {
+                if (cudaGraphLaunch(ex, origin) != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "batch launch failed");
+            }
+            if (ex) {
+                cudaStreamSynchronize(origin);
+                cudaGraphExecDestroy(ex);
+            }
+        }
+    }
+    // stopping rules that read the error back: round-robin, one iteration at a time
+    bool any = true;
+    while (rc == DWCU_SUCCESS && any) {
+        any = false;
+        for (int i : rel_idx) {
+            dwcu_job *j = jobs[i];
+            if (j->finished) continue;
+            if (rc == DWCU_SUCCESS) rc = job_step_impl(j, 1, nullptr);
+            any = any || !j->finished;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        cudaStreamSynchronize(streams[(size_t) i]);
+        jobs[i]->stream = saved[(size_t) i];
+        cudaStreamDestroy(streams[(size_t) i]);
+    }
+    cudaStreamSynchronize(origin);
+    cudaEventDestroy(fork);
+    cudaEventDestroy(done);
+    return rc;
+}
+
 static int one_call(const float *im, long long M, long long N, long long P, const float *psf, long long pM,
                     long long pN, long long pP, dwcu_opts *s, float *out, bool on_device, cudaStream_t stream)
 {
@@ -1228,6 +1334,12 @@ int dwcu_job_step(dwcu_job *job, int32_t n, int32_t *remaining)
 {
     if (!job) return fail(DWCU_ERROR_INVALID_VALUE, "job is NULL");
     return job_step(job, n, remaining);
+}
+
+int dwcu_batch_run(dwcu_job **jobs, int32_t n, void *stream)
+{
+    if (!jobs && n > 0) return fail(DWCU_ERROR_INVALID_VALUE, "jobs is NULL");
+    return batch_run(jobs, n, (cudaStream_t) stream);
 }
 
 int dwcu_job_done(const dwcu_job *job) { return job && job->finished ? 1 : 0; }

@@ -1,0 +1,414 @@
+// host.cu -- the parts of dw_run around the iteration: PSF preparation and
+// tiled deconvolution with all tiles batched on the GPU.
+//
+//   dwcu_psf_prepare      fim_normalize_sum1 (src/fim.c:900-912) and
+//                         psf_autocrop (src/dw.c:1764-1997)
+//   dwcu_tiling_create    tiling_getDivision / tiling_create (src/tiling.c:22-130)
+//   dwcu_deconvolve_tiled deconvolve_tiles (src/dw.c:2001-2229) without the
+//                         temporary raw files: the image stays on the device,
+//                         tiles become jobs that iterate as one batch, and the
+//                         weighted blend of tiling_put_tile (src/tiling.c:412-439)
+//                         runs as a device kernel per tile, in tile order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dwcu.h"
+
+namespace dwcu {
+void record_error(const char *msg);  // engine.cu: the text dwcu_last_error returns
+void record_launch();                // engine.cu: dwcu_launch_count
+}  // namespace dwcu
+
+namespace dwcu_host {
+
+static int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    dwcu::record_error(buf);
+    return code;
+}
+
+#define HCU(call)                                                                                      \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail(e_ == cudaErrorMemoryAllocation ? DWCU_ERROR_OUT_OF_MEMORY : DWCU_ERROR_CUDA,  \
+                        "%s failed: %s", #call, cudaGetErrorString(e_));                               \
+    } while (0)
+
+// ------------------------------------------------------------ PSF preparation
+
+// fim_normalize_sum1, fim.c:900-912: divide by the double sum
+static void normalize_sum1(std::vector<float> &p)
+{
+    double s = 0;
+    for (float v : p) s += v;
+    for (float &v : p) v = (float) (v / s);
+}
+
+// fim_get_cuboid, fim.c:659-693
+static std::vector<float> cuboid(const std::vector<float> &A, int64_t M, int64_t N, int64_t m0, int64_t m1,
+                                 int64_t n0, int64_t n1, int64_t p0, int64_t p1)
+{
+    const int64_t m = m1 - m0 + 1, n = n1 - n0 + 1, p = p1 - p0 + 1;
+    std::vector<float> C((size_t) (m * n * p));
+    for (int64_t cc = p0; cc <= p1; ++cc)
+        for (int64_t bb = n0; bb <= n1; ++bb)
+            for (int64_t aa = m0; aa <= m1; ++aa)
+                C[(size_t) ((aa - m0) + (bb - n0) * m + (cc - p0) * m * n)] = A[(size_t) (aa + bb * M + cc * M * N)];
+    return C;
+}
+
+// psf_autocrop_byImage, dw.c:1764-1860
+static void crop_by_image(std::vector<float> &psf, int64_t &pM, int64_t &pN, int64_t &pP, int64_t M, int64_t N,
+                          int64_t P, int bq)
+{
+    int64_t mopt = (M - 1) * 2 + 1, nopt = (N - 1) * 2 + 1, popt = (P - 1) * 2 + 1;
+    if (bq == 0) {
+        mopt = M;
+        nopt = N;
+        popt = P;
+    }
+    if (pP < popt) return;  // the reference warns that the PSF has too few slices
+    if (pM > mopt || pN > nopt || pP > popt) {
+        int64_t m0 = 0, m1 = pM - 1, n0 = 0, n1 = pN - 1, p0 = 0, p1 = pP - 1;
+        if (pM > mopt) { m0 = (pM - mopt) / 2; m1 = m1 - (pM - mopt) / 2; }
+        if (pN > nopt) { n0 = (pN - nopt) / 2; n1 = n1 - (pN - nopt) / 2; }
+        if (pP > popt) { p0 = (pP - popt) / 2; p1 = p1 - (pP - popt) / 2; }
+        psf = cuboid(psf, pM, pN, m0, m1, n0, n1, p0, p1);
+        pM = m1 - m0 + 1;
+        pN = n1 - n0 + 1;
+        pP = p1 - p0 + 1;
+    }
+}
+
+// psf_autocrop_XY, dw.c:1862-1971 (without the FFTW lookahead benchmark):
+// drop outer x (and as many y) planes whose y-z sum is below
+// xycropfactor times the largest one; float sums as in the reference
+static void crop_xy(std::vector<float> &psf, int64_t &pM, int64_t &pN, int64_t pP, float xycropfactor)
+{
+    float maxsum = 0;
+    for (int64_t xx = 0; xx < pM; ++xx) {
+        float sum = 0;
+        for (int64_t yy = 0; yy < pN; ++yy)
+            for (int64_t zz = 0; zz < pP; ++zz) sum += psf[(size_t) (xx + yy * pM + zz * pM * pN)];
+        if (sum > maxsum) maxsum = sum;
+    }
+    int64_t first = -1;
+    float sum = 0;
+    while (sum < xycropfactor * maxsum && first + 1 < pM) {
+        first++;
+        sum = 0;
+        for (int64_t yy = 0; yy < pN; ++yy)
+            for (int64_t zz = 0; zz < pP; ++zz) sum += psf[(size_t) (first + yy * pM + zz * pM * pN)];
+    }
+    if (first < 1) return;
+    if (pM - 2 * first < 1 || pN - 2 * first < 1) return;
+    psf = cuboid(psf, pM, pN, first, pM - first - 1, first, pN - first - 1, 0, pP - 1);
+    pM -= 2 * first;
+    pN -= 2 * first;
+}
+
+}  // namespace dwcu_host
+
+using namespace dwcu_host;
+
+// ------------------------------------------------------------ tiling kernels
+
+namespace {
+
+struct DevTile {
+    long long pos[6], xpos[6], xsize[3];
+};
+
+// getWeight1d, tiling.c:169-197 (float arithmetic as in the reference)
+__host__ __device__ inline float weight1d(float a, float b, float c, float d, long long x)
+{
+    const float xf = (float) x;
+    if (xf < a || xf > d) return 0.f;
+    if (xf >= b && xf <= c) return 1.f;
+    if (xf >= a && xf <= b) return (xf - a + 1) / (b - a + 1);
+    if (xf >= c && xf <= d) return 1 - (xf - c) / (d - c + 1);
+    return 0.f;
+}
+
+// tile_getWeight, tiling.c:199-216
+__host__ __device__ inline float tile_weight(const DevTile &t, long long m, long long n)
+{
+    const float wm = weight1d((float) t.xpos[0], (float) t.pos[0], (float) t.pos[1], (float) t.xpos[1], m);
+    const float wn = weight1d((float) t.xpos[2], (float) t.pos[2], (float) t.pos[3], (float) t.xpos[3], n);
+    return fminf(wm, wn);
+}
+
+// tiling_get_tile (tiling.c:318-351) plus the offset dw.c adds per tile
+__global__ void k_tile_extract(const float *__restrict__ im, long long M, long long N, DevTile t, float offset,
+                               float *__restrict__ out)
+{
+    const long long m = t.xsize[0], n = t.xsize[1], p = t.xsize[2];
+    const long long total = m * n * p;
+    for (long long k = blockIdx.x * (long long) blockDim.x + threadIdx.x; k < total;
+         k += (long long) gridDim.x * blockDim.x) {
+        const long long a = k % m, b = (k / m) % n, c = k / (m * n);
+        float v = im[(a + t.xpos[0]) + (b + t.xpos[2]) * M + (c + t.xpos[4]) * M * N];
+        if (offset > 0) v += offset;
+        out[k] = v;
+    }
+}
+
+// minus the offset, project positive (dw.c:2141-2145), then tiling_put_tile
+// (tiling.c:412-439): V += w / sum_w * S, tiles in order
+__global__ void k_tile_blend(const float *__restrict__ S, long long M, long long N, const DevTile *__restrict__ tiles,
+                             int ntiles, int tid, float offset, float *__restrict__ V)
+{
+    const DevTile t = tiles[tid];
+    const long long m = t.xsize[0], n = t.xsize[1], p = t.xsize[2];
+    const long long total = m * n * p;
+    for (long long k = blockIdx.x * (long long) blockDim.x + threadIdx.x; k < total;
+         k += (long long) gridDim.x * blockDim.x) {
+        const long long a = k % m, b = (k / m) % n, c = k / (m * n);
+        const long long aa = a + t.xpos[0], bb = b + t.xpos[2], cc = c + t.xpos[4];
+        float s = S[k];
+        if (offset > 0) {
+            s = __fadd_rn(s, -offset);
+            if (s < 0) s = 0;
+        }
+        float w = tile_weight(t, aa, bb);
+        float ws = 0;
+        for (int q = 0; q < ntiles; ++q) ws = __fadd_rn(ws, tile_weight(tiles[q], aa, bb));
+        w = __fdiv_rn(w, ws);
+        float &v = V[aa + bb * M + cc * M * N];
+        v = __fadd_rn(v, __fmul_rn(w, s));  // no contraction: the CPU blend rounds twice
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ C ABI
+
+extern "C" {
+
+int dwcu_psf_prepare(const float *psf, int64_t pM, int64_t pN, int64_t pP, int64_t M, int64_t N, int64_t P,
+                     int32_t border_quality, float xycropfactor, float *out, int64_t out_dims[3])
+{
+    if (!psf || !out || !out_dims) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    if (pM < 1 || pN < 1 || pP < 1 || M < 1 || N < 1 || P < 1) return fail(DWCU_ERROR_INVALID_VALUE, "bad sizes");
+    std::vector<float> p(psf, psf + pM * pN * pP);
+    normalize_sum1(p);                                          // dw.c:2799
+    crop_by_image(p, pM, pN, pP, M, N, P, border_quality);      // dw.c:1985-1988
+    if (border_quality > 0 && xycropfactor > 0) crop_xy(p, pM, pN, pP, xycropfactor);  // dw.c:1990-1996
+    normalize_sum1(p);                                          // dw.c:2826
+    memcpy(out, p.data(), sizeof(float) * p.size());
+    out_dims[0] = pM;
+    out_dims[1] = pN;
+    out_dims[2] = pP;
+    return DWCU_SUCCESS;
+}
+
+int dwcu_tiling_create(int64_t M, int64_t N, int64_t P, int64_t max_size, int64_t overlap, dwcu_tile *tiles,
+                       int32_t capacity, int32_t *ntiles)
+{
+    if (M < 1 || N < 1 || P < 1 || max_size < 1 || overlap < 0 || !ntiles)
+        return fail(DWCU_ERROR_INVALID_VALUE, "bad tiling arguments");
+    // tiling_getDivision, tiling.c:22-58 (float section width as in the reference)
+    auto division = [](int64_t L, int64_t m, std::vector<int64_t> &divs) {
+        const float ns = (float) std::ceil((double) L / (double) m);
+        const float width = (float) L / ns;
+        const int64_t n = (int64_t) ns;
+        divs.assign((size_t) (2 * n), 0);
+        divs[0] = 0;
+        divs[(size_t) (2 * n - 1)] = L - 1;
+        for (int64_t dd = 1; dd < n; ++dd) {
+            divs[(size_t) (dd * 2 - 1)] = (int64_t) std::ceil(width * (float) dd) - 1;
+            divs[(size_t) (dd * 2)] = divs[(size_t) (dd * 2 - 1)] + 1;
+        }
+        return n;
+    };
+    std::vector<int64_t> dM, dN;
+    const int64_t nM = division(M, max_size, dM), nN = division(N, max_size, dN);
+    *ntiles = (int32_t) (nM * nN);
+    if (!tiles) return DWCU_SUCCESS;
+    if (capacity < nM * nN) return fail(DWCU_ERROR_INVALID_VALUE, "tile array too small (%lld)", (long long) (nM * nN));
+    int b = 0;
+    for (int64_t mm = 0; mm < nM; ++mm)  // tiling.c:95-128
+        for (int64_t nn = 0; nn < nN; ++nn, ++b) {
+            dwcu_tile &t = tiles[b];
+            t.size[0] = dM[(size_t) (mm * 2 + 1)] - dM[(size_t) (mm * 2)] + 1;
+            t.size[1] = dN[(size_t) (nn * 2 + 1)] - dN[(size_t) (nn * 2)] + 1;
+            t.size[2] = P;
+            t.pos[0] = dM[(size_t) (mm * 2)]; t.pos[1] = dM[(size_t) (mm * 2 + 1)];
+            t.pos[2] = dN[(size_t) (nn * 2)]; t.pos[3] = dN[(size_t) (nn * 2 + 1)];
+            t.pos[4] = 0; t.pos[5] = P - 1;
+            t.xpos[0] = std::max<int64_t>(0, t.pos[0] - overlap);
+            t.xpos[1] = std::min<int64_t>(t.pos[1] + overlap, M - 1);
+            t.xpos[2] = std::max<int64_t>(0, t.pos[2] - overlap);
+            t.xpos[3] = std::min<int64_t>(t.pos[3] + overlap, N - 1);
+            t.xpos[4] = t.pos[4]; t.xpos[5] = t.pos[5];
+            t.xsize[0] = t.xpos[1] - t.xpos[0] + 1;
+            t.xsize[1] = t.xpos[3] - t.xpos[2] + 1;
+            t.xsize[2] = t.xpos[5] - t.xpos[4] + 1;
+        }
+    return DWCU_SUCCESS;
+}
+
+int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, const float *psf, int64_t pM,
+                          int64_t pN, int64_t pP, int64_t tile_size, int64_t overlap, float offset,
+                          float xycropfactor, double hbm_budget, dwcu_opts *s, float *out)
+{
+    if (!im || !psf || !out || !s) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    int32_t nt = 0;
+    int rc = dwcu_tiling_create(M, N, P, tile_size, overlap, nullptr, 0, &nt);
+    if (rc) return rc;
+    if (nt < 2) return fail(DWCU_ERROR_INVALID_VALUE, "only one tile: omit the tile size or decrease it");
+    std::vector<dwcu_tile> tiles((size_t) nt);
+    dwcu_tiling_create(M, N, P, tile_size, overlap, tiles.data(), nt, &nt);
+    HCU(cudaSetDevice(s->device));
+    cudaStream_t st = nullptr;
+    HCU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const size_t nvox = (size_t) (M * N * P);
+    float *d_im = nullptr, *d_out = nullptr;
+    DevTile *d_tiles = nullptr;
+    std::vector<DevTile> ht((size_t) nt);
+    for (int i = 0; i < nt; ++i) {
+        memcpy(ht[(size_t) i].pos, tiles[(size_t) i].pos, sizeof ht[0].pos);
+        memcpy(ht[(size_t) i].xpos, tiles[(size_t) i].xpos, sizeof ht[0].xpos);
+        memcpy(ht[(size_t) i].xsize, tiles[(size_t) i].xsize, sizeof ht[0].xsize);
+    }
+    auto cleanup = [&]() {
+        if (d_im) cudaFree(d_im);
+        if (d_out) cudaFree(d_out);
+        if (d_tiles) cudaFree(d_tiles);
+        if (st) cudaStreamDestroy(st);
+    };
+#define TCU(call)                                                                       \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            cleanup();                                                                  \
+            return fail(e_ == cudaErrorMemoryAllocation ? DWCU_ERROR_OUT_OF_MEMORY : DWCU_ERROR_CUDA, \
+                        "%s failed: %s", #call, cudaGetErrorString(e_));                \
+        }                                                                               \
+    } while (0)
+    TCU(cudaMalloc(&d_im, sizeof(float) * nvox));
+    TCU(cudaMalloc(&d_out, sizeof(float) * nvox));
+    TCU(cudaMalloc(&d_tiles, sizeof(DevTile) * (size_t) nt));
+    TCU(cudaMemcpyAsync(d_im, im, sizeof(float) * nvox, cudaMemcpyHostToDevice, st));
+    TCU(cudaMemcpyAsync(d_tiles, ht.data(), sizeof(DevTile) * (size_t) nt, cudaMemcpyHostToDevice, st));
+    TCU(cudaMemsetAsync(d_out, 0, sizeof(float) * nvox, st));
+
+    // per tile: PSF copy normalised and cropped against the tile (dw.c:2112-2130)
+    struct TileJob {
+        dwcu_job *job = nullptr;
+        std::vector<float> psf;
+        int64_t d[3] = {0, 0, 0};
+        float *d_tile = nullptr;
+        float *d_psf = nullptr;
+    };
+    std::vector<TileJob> tj((size_t) nt);
+    for (int i = 0; i < nt; ++i) {
+        TileJob &T = tj[(size_t) i];
+        const dwcu_tile &t = tiles[(size_t) i];
+        T.psf.assign(psf, psf + pM * pN * pP);
+        int64_t a = pM, b = pN, c = pP;
+        normalize_sum1(T.psf);
+        crop_by_image(T.psf, a, b, c, t.xsize[0], t.xsize[1], t.xsize[2], s->border_quality);
+        if (s->border_quality > 0 && xycropfactor > 0) crop_xy(T.psf, a, b, c, xycropfactor);
+        normalize_sum1(T.psf);
+        T.d[0] = a; T.d[1] = b; T.d[2] = c;
+    }
+    // waves of tiles that fit the device-memory budget, each run as one batch
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const double budget = hbm_budget > 0 ? hbm_budget : 0.85 * (double) free_b;
+    int next = 0;
+    rc = DWCU_SUCCESS;
+    std::vector<float> trace_acc;
+    while (next < nt && rc == DWCU_SUCCESS) {
+        std::vector<int> wave;
+        double used = 0;
+        for (int i = next; i < nt; ++i) {
+            const dwcu_tile &t = tiles[(size_t) i];
+            int64_t w3[3];
+            int64_t need = 0;
+            rc = dwcu_plan_size(t.xsize[0], t.xsize[1], t.xsize[2], tj[(size_t) i].d[0], tj[(size_t) i].d[1],
+                                tj[(size_t) i].d[2], s->border_quality, s->method, w3, &need);
+            if (rc) break;
+            need += (int64_t) (sizeof(float) * (t.xsize[0] * t.xsize[1] * t.xsize[2]) * 2);
+            if (!wave.empty() && used + (double) need > budget) break;
+            used += (double) need;
+            wave.push_back(i);
+        }
+        if (rc) break;
+        std::vector<dwcu_job *> jobs;
+        for (int i : wave) {
+            TileJob &T = tj[(size_t) i];
+            const dwcu_tile &t = tiles[(size_t) i];
+            const size_t tv = (size_t) (t.xsize[0] * t.xsize[1] * t.xsize[2]);
+            if (cudaMalloc(&T.d_tile, sizeof(float) * tv) != cudaSuccess ||
+                cudaMalloc(&T.d_psf, sizeof(float) * T.psf.size()) != cudaSuccess) {
+                rc = fail(DWCU_ERROR_OUT_OF_MEMORY, "tile buffers");
+                break;
+            }
+            cudaMemcpyAsync(T.d_psf, T.psf.data(), sizeof(float) * T.psf.size(), cudaMemcpyHostToDevice, st);
+            const int blocks = (int) std::min<size_t>(4096, (tv + 255) / 256);
+            k_tile_extract<<<blocks, 256, 0, st>>>(d_im, M, N, ht[(size_t) i], offset, T.d_tile);
+            dwcu::record_launch();
+            cudaStreamSynchronize(st);
+            rc = dwcu_job_create(t.xsize[0], t.xsize[1], t.xsize[2], T.d[0], T.d[1], T.d[2], s, &T.job);
+            if (rc == DWCU_SUCCESS) rc = dwcu_job_setup(T.job, T.d_tile, T.d_psf, 1);
+            if (rc) break;
+            jobs.push_back(T.job);
+        }
+        if (rc == DWCU_SUCCESS) rc = dwcu_batch_run(jobs.data(), (int32_t) jobs.size(), st);
+        // results in tile order, blended on the device
+        for (int i : wave) {
+            TileJob &T = tj[(size_t) i];
+            const dwcu_tile &t = tiles[(size_t) i];
+            const size_t tv = (size_t) (t.xsize[0] * t.xsize[1] * t.xsize[2]);
+            if (rc == DWCU_SUCCESS && T.job) {
+                dwcu_opts so;
+                dwcu_opts_init(&so);
+                so.error_trace = nullptr;
+                rc = dwcu_job_result(T.job, T.d_tile, 1, &so);
+                if (rc == DWCU_SUCCESS) {
+                    s->iterations_done = so.iterations_done;
+                    const int blocks = (int) std::min<size_t>(4096, (tv + 255) / 256);
+                    k_tile_blend<<<blocks, 256, 0, st>>>(T.d_tile, M, N, d_tiles, nt, i, offset, d_out);
+                    dwcu::record_launch();
+                    cudaStreamSynchronize(st);
+                }
+            }
+            if (T.job) dwcu_job_destroy(T.job);
+            T.job = nullptr;
+            if (T.d_tile) cudaFree(T.d_tile);
+            if (T.d_psf) cudaFree(T.d_psf);
+            T.d_tile = T.d_psf = nullptr;
+        }
+        next = wave.empty() ? nt : wave.back() + 1;
+    }
+    if (rc == DWCU_SUCCESS) {
+        cudaError_t e = cudaMemcpyAsync(out, d_out, sizeof(float) * nvox, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "result copy failed: %s", cudaGetErrorString(e));
+    }
+    for (auto &T : tj) {
+        if (T.job) dwcu_job_destroy(T.job);
+        if (T.d_tile) cudaFree(T.d_tile);
+        if (T.d_psf) cudaFree(T.d_psf);
+    }
+    cleanup();
+#undef TCU
+    return rc;
+}
+
+}  // extern "C"

@@ -131,6 +131,13 @@ int dwcu_job_setup(dwcu_job *job, const float *im, const float *psf, int32_t on_
  * s->iter_type is applied; REL and ABS read each error back (one small copy
  * per iteration).  *remaining receives how many iterations may still run. */
 int dwcu_job_step(dwcu_job *job, int32_t n, int32_t *remaining);
+/* Run set-up jobs to completion together: jobs with a fixed iteration count
+ * become independent chains of one CUDA graph (one stream each), so tiles
+ * and channels of uneven sizes share the GPU; REL/ABS jobs are stepped
+ * round-robin.  Replaces the sequential tile loop of deconvolve_tiles
+ * (src/dw.c:2093-2153) for the iteration part.  Returns when all are done;
+ * results are then read with dwcu_job_result. */
+int dwcu_batch_run(dwcu_job **jobs, int32_t n, void *stream);
 /* 1 when the job has finished all its iterations. */
 int dwcu_job_done(const dwcu_job *job);
 /* Wait for the job's queued work; copy the result (host or device pointer)
@@ -142,6 +149,53 @@ void dwcu_job_destroy(dwcu_job *job);
 int dwcu_job_set_stream(dwcu_job *job, void *stream);
 /* Device bytes held by the job. */
 int64_t dwcu_job_bytes(const dwcu_job *job);
+
+/* ---------------------------------------------------------------- PSF and tiles */
+
+/* Prepare a PSF for an M x N x P job the way dw_run does before the method
+ * call (src/dw.c:2797-2826 with psf_autocrop, src/dw.c:1973-1997): normalise
+ * to sum 1 (fim_normalize_sum1, src/fim.c:900-912), crop to at most
+ * 2*size-1 per axis (size with border_quality 0; psf_autocrop_byImage,
+ * src/dw.c:1764-1860), drop outer x/y planes holding less than xycropfactor
+ * of the largest y-z plane sum (border_quality > 0 only; psf_autocrop_XY
+ * without the FFT lookahead, src/dw.c:1862-1971), normalise again.  out must
+ * hold pM*pN*pP floats; out_dims receives the new size. */
+int dwcu_psf_prepare(const float *psf, int64_t pM, int64_t pN, int64_t pP,
+                     int64_t M, int64_t N, int64_t P, int32_t border_quality,
+                     float xycropfactor, float *out, int64_t out_dims[3]);
+
+/* One tile of a tiling (struct tile, src/tiling.h:29-34): the owned region
+ * pos = [m0, m1, n0, n1, p0, p1] and the region deconvolved xpos (pos grown
+ * by the overlap and clipped to the image), with their sizes. */
+typedef struct dwcu_tile {
+    int64_t size[3];
+    int64_t pos[6];
+    int64_t xpos[6];
+    int64_t xsize[3];
+} dwcu_tile;
+
+/* The tiling tiling_create(M, N, P, max_size, overlap) builds (src/tiling.c:
+ * 22-130): x and y cut into ceil(L / max_size) near-equal sections, tiles
+ * ordered x-section outer, y-section inner.  *ntiles receives the count;
+ * tiles (capacity entries, may be NULL to query the count) the tiles. */
+int dwcu_tiling_create(int64_t M, int64_t N, int64_t P, int64_t max_size, int64_t overlap,
+                       dwcu_tile *tiles, int32_t capacity, int32_t *ntiles);
+
+/* Tiled deconvolution, deconvolve_tiles (src/dw.c:2001-2229) with the image
+ * and the result in memory instead of temporary raw files: im and out are
+ * host M x N x P buffers, psf the PSF as deconvolve_tiles receives it (from
+ * dw_run, already normalised and cropped against the whole image).  Per tile
+ * the PSF is normalised, cropped against the tile and normalised again, the
+ * tile gets +offset (when offset > 0), is deconvolved with options s, gets
+ * -offset and is clipped at 0, and is blended into out with the weights of
+ * tiling_put_tile (src/tiling.c:412-439), in tile order.  The tiles run as
+ * batches (dwcu_batch_run) of as many tiles as fit hbm_budget bytes (<= 0:
+ * 85 % of the free device memory).  Fails with DWCU_ERROR_INVALID_VALUE for a
+ * tiling of one tile, as the reference does. */
+int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P,
+                          const float *psf, int64_t pM, int64_t pN, int64_t pP,
+                          int64_t tile_size, int64_t overlap, float offset, float xycropfactor,
+                          double hbm_budget, dwcu_opts *s, float *out);
 
 /* ---------------------------------------------------------------- FFT */
 

@@ -425,3 +425,215 @@ int dwo_deconvolve(const float *im, i64 M, i64 N, i64 P,
     free(K); free(C); free(Z); free(W); free(x); free(xp); free(xn);
     return 0;
 }
+
+/* ================================================ PSF preparation, tiling */
+
+/* fim_normalize_sum1, src/fim.c:900-912 (serial double sum) */
+static void normalize_sum1(float *p, size_t n)
+{
+    double s = 0;
+    for (size_t k = 0; k < n; k++) s += p[k];
+    for (size_t k = 0; k < n; k++) p[k] = (float) (p[k] / s);
+}
+
+/* fim_get_cuboid, src/fim.c:659-693, into a new buffer */
+static float *cuboid(const float *A, i64 M, i64 N, i64 m0, i64 m1, i64 n0, i64 n1, i64 p0, i64 p1)
+{
+    i64 m = m1 - m0 + 1, n = n1 - n0 + 1, p = p1 - p0 + 1;
+    float *C = malloc(sizeof(float) * (size_t) (m * n * p));
+    for (i64 cc = p0; cc <= p1; cc++)
+        for (i64 bb = n0; bb <= n1; bb++)
+            for (i64 aa = m0; aa <= m1; aa++)
+                C[(aa - m0) + (bb - n0) * m + (cc - p0) * m * n] = A[aa + bb * M + cc * M * N];
+    return C;
+}
+
+/* psf_autocrop, src/dw.c:1973-1997: psf_autocrop_byImage (dw.c:1764-1860)
+ * and, for bq > 0 and xycropfactor > 0, psf_autocrop_XY without the FFT
+ * lookahead (dw.c:1862-1971).  Takes ownership of psf (malloc'd). */
+float *dwo_psf_autocrop(float *psf, i64 *pM, i64 *pN, i64 *pP, i64 M, i64 N, i64 P, int bq,
+                        float xycropfactor)
+{
+    i64 m = *pM, n = *pN, p = *pP;
+    i64 mopt = (M - 1) * 2 + 1, nopt = (N - 1) * 2 + 1, popt = (P - 1) * 2 + 1;
+    if (bq == 0) { mopt = M; nopt = N; popt = P; }
+    if (p < popt) return psf; /* the reference warns and returns before the XY crop */
+    if (m > mopt || n > nopt || p > popt) {
+        i64 m0 = 0, m1 = m - 1, n0 = 0, n1 = n - 1, p0 = 0, p1 = p - 1;
+        if (m > mopt) { m0 = (m - mopt) / 2; m1 = m1 - (m - mopt) / 2; }
+        if (n > nopt) { n0 = (n - nopt) / 2; n1 = n1 - (n - nopt) / 2; }
+        if (p > popt) { p0 = (p - popt) / 2; p1 = p1 - (p - popt) / 2; }
+        float *c = cuboid(psf, m, n, m0, m1, n0, n1, p0, p1);
+        free(psf);
+        psf = c;
+        *pM = m = m1 - m0 + 1;
+        *pN = n = n1 - n0 + 1;
+        *pP = p = p1 - p0 + 1;
+    }
+    if (bq <= 0 || xycropfactor <= 0) return psf;
+    float maxsum = 0;
+    for (i64 xx = 0; xx < m; xx++) {
+        float sum = 0;
+        for (i64 yy = 0; yy < n; yy++)
+            for (i64 zz = 0; zz < p; zz++) sum += psf[xx + yy * m + zz * m * n];
+        if (sum > maxsum) maxsum = sum;
+    }
+    i64 first = -1;
+    float sum = 0;
+    while (sum < xycropfactor * maxsum && first + 1 < m) {
+        first++;
+        sum = 0;
+        for (i64 yy = 0; yy < n; yy++)
+            for (i64 zz = 0; zz < p; zz++) sum += psf[first + yy * m + zz * m * n];
+    }
+    if (first < 1 || m - 2 * first < 1 || n - 2 * first < 1) return psf;
+    float *c = cuboid(psf, m, n, first, m - first - 1, first, n - first - 1, 0, p - 1);
+    free(psf);
+    *pM = m - 2 * first;
+    *pN = n - 2 * first;
+    return c;
+}
+
+int dwo_psf_prepare(const float *psf, i64 pM, i64 pN, i64 pP, i64 M, i64 N, i64 P, int bq,
+                    float xycropfactor, float *out, i64 out_dims[3])
+{
+    float *p = malloc(sizeof(float) * (size_t) (pM * pN * pP));
+    memcpy(p, psf, sizeof(float) * (size_t) (pM * pN * pP));
+    normalize_sum1(p, (size_t) (pM * pN * pP));                 /* dw.c:2799 */
+    p = dwo_psf_autocrop(p, &pM, &pN, &pP, M, N, P, bq, xycropfactor);
+    normalize_sum1(p, (size_t) (pM * pN * pP));                 /* dw.c:2826 */
+    memcpy(out, p, sizeof(float) * (size_t) (pM * pN * pP));
+    free(p);
+    out_dims[0] = pM; out_dims[1] = pN; out_dims[2] = pP;
+    return 0;
+}
+
+/* tiling_getDivision, src/tiling.c:22-58 (float section width) */
+static i64 division(i64 L, i64 m, i64 *divs /* 2 * ceil(L/m) */)
+{
+    float ns = (float) ceil((double) L / (double) m);
+    float width = (float) L / ns;
+    i64 n = (i64) ns;
+    divs[0] = 0;
+    divs[2 * n - 1] = L - 1;
+    for (i64 dd = 1; dd < n; dd++) {
+        divs[dd * 2 - 1] = (i64) ceilf(width * (float) dd) - 1;
+        divs[dd * 2] = divs[dd * 2 - 1] + 1;
+    }
+    return n;
+}
+
+/* tiling_create, src/tiling.c:70-130.  Each tile is 18 int64: size[3],
+ * pos[6], xpos[6], xsize[3].  Returns the tile count (tiles may be NULL). */
+int dwo_tiling_create(i64 M, i64 N, i64 P, i64 max_size, i64 overlap, i64 *tiles, int capacity)
+{
+    i64 nM0 = (i64) ceil((double) M / (double) max_size), nN0 = (i64) ceil((double) N / (double) max_size);
+    i64 *dM = calloc((size_t) (2 * nM0), sizeof(i64)), *dN = calloc((size_t) (2 * nN0), sizeof(i64));
+    i64 nM = division(M, max_size, dM), nN = division(N, max_size, dN);
+    int nt = (int) (nM * nN);
+    if (tiles && capacity >= nt) {
+        int b = 0;
+        for (i64 mm = 0; mm < nM; mm++)
+            for (i64 nn = 0; nn < nN; nn++, b++) {
+                i64 *t = tiles + 18 * b, *size = t, *pos = t + 3, *xpos = t + 9, *xsize = t + 15;
+                size[0] = dM[mm * 2 + 1] - dM[mm * 2] + 1;
+                size[1] = dN[nn * 2 + 1] - dN[nn * 2] + 1;
+                size[2] = P;
+                pos[0] = dM[mm * 2]; pos[1] = dM[mm * 2 + 1];
+                pos[2] = dN[nn * 2]; pos[3] = dN[nn * 2 + 1];
+                pos[4] = 0; pos[5] = P - 1;
+                xpos[0] = pos[0] - overlap > 0 ? pos[0] - overlap : 0;
+                xpos[1] = pos[1] + overlap < M - 1 ? pos[1] + overlap : M - 1;
+                xpos[2] = pos[2] - overlap > 0 ? pos[2] - overlap : 0;
+                xpos[3] = pos[3] + overlap < N - 1 ? pos[3] + overlap : N - 1;
+                xpos[4] = pos[4]; xpos[5] = pos[5];
+                xsize[0] = xpos[1] - xpos[0] + 1;
+                xsize[1] = xpos[3] - xpos[2] + 1;
+                xsize[2] = xpos[5] - xpos[4] + 1;
+            }
+    }
+    free(dM);
+    free(dN);
+    return nt;
+}
+
+/* getWeight1d, src/tiling.c:169-197 */
+static float weight1d(float a, float b, float c, float d, i64 x)
+{
+    if (x < a || x > d) return 0;
+    if (x >= b && x <= c) return 1;
+    if (x >= a && x <= b) return (x - a + 1) / (b - a + 1);
+    if (x >= c && x <= d) return 1 - (x - c) / (d - c + 1);
+    return -1;
+}
+
+/* tile_getWeight, src/tiling.c:199-216 */
+float dwo_tile_weight(const i64 *t, i64 m, i64 n)
+{
+    const i64 *pos = t + 3, *xpos = t + 9;
+    float wm = weight1d(xpos[0], pos[0], pos[1], xpos[1], m);
+    float wn = weight1d(xpos[2], pos[2], pos[3], xpos[3], n);
+    return fminf(wm, wn);
+}
+
+/* deconvolve_tiles, src/dw.c:2001-2229, in memory: tiles by tiling_get_tile
+ * (tiling.c:318-351), per-tile PSF normalise / autocrop / normalise
+ * (dw.c:2124-2130), +offset, the method, -offset and projection
+ * (dw.c:2132-2145), blended with tiling_put_tile (tiling.c:412-439).
+ * s->iterations_done receives the last tile's count.  Returns 0, or a
+ * negative code (one tile only: -3). */
+int dwo_deconvolve_tiled(const float *im, i64 M, i64 N, i64 P, const float *psf, i64 pM, i64 pN, i64 pP,
+                         i64 tile_size, i64 overlap, float offset, float xycropfactor, dwo_opts *s, float *out)
+{
+    int nt = dwo_tiling_create(M, N, P, tile_size, overlap, NULL, 0);
+    if (nt < 2) return -3;
+    i64 *tiles = malloc(sizeof(i64) * 18 * (size_t) nt);
+    dwo_tiling_create(M, N, P, tile_size, overlap, tiles, nt);
+    memset(out, 0, sizeof(float) * (size_t) (M * N * P));
+    int rc = 0;
+    for (int tt = 0; tt < nt && rc == 0; tt++) {
+        const i64 *t = tiles + 18 * tt, *xpos = t + 9, *xsize = t + 15;
+        i64 m = xsize[0], n = xsize[1], p = xsize[2];
+        size_t tv = (size_t) (m * n * p);
+        float *tile = malloc(sizeof(float) * tv);
+        for (i64 cc = 0; cc < p; cc++)
+            for (i64 bb = 0; bb < n; bb++)
+                for (i64 aa = 0; aa < m; aa++)
+                    tile[aa + bb * m + cc * m * n] = im[(aa + xpos[0]) + (bb + xpos[2]) * M + (cc + xpos[4]) * M * N];
+        i64 a = pM, b = pN, c = pP;
+        float *tp = malloc(sizeof(float) * (size_t) (a * b * c));
+        memcpy(tp, psf, sizeof(float) * (size_t) (a * b * c));
+        normalize_sum1(tp, (size_t) (a * b * c));
+        tp = dwo_psf_autocrop(tp, &a, &b, &c, m, n, p, s->border_quality, xycropfactor);
+        normalize_sum1(tp, (size_t) (a * b * c));
+        if (offset > 0)
+            for (size_t k = 0; k < tv; k++) tile[k] += offset;
+        float *res = malloc(sizeof(float) * tv);
+        dwo_opts so = *s;
+        so.error_trace = NULL;
+        so.trace_capacity = 0;
+        rc = dwo_deconvolve(tile, m, n, p, tp, a, b, c, &so, res);
+        s->iterations_done = so.iterations_done;
+        if (rc == 0) {
+            if (offset > 0)
+                for (size_t k = 0; k < tv; k++) {
+                    res[k] += -offset;
+                    if (res[k] < 0) res[k] = 0;
+                }
+            for (i64 cc = xpos[4]; cc <= xpos[5]; cc++)
+                for (i64 bb = xpos[2]; bb <= xpos[3]; bb++)
+                    for (i64 aa = xpos[0]; aa <= xpos[1]; aa++) {
+                        float w = dwo_tile_weight(t, aa, bb);
+                        float ws = 0;
+                        for (int q = 0; q < nt; q++) ws += dwo_tile_weight(tiles + 18 * q, aa, bb);
+                        w /= ws;
+                        out[aa + bb * M + cc * M * N] += w * res[(aa - xpos[0]) + (bb - xpos[2]) * m + (cc - xpos[4]) * m * n];
+                    }
+        }
+        free(res);
+        free(tp);
+        free(tile);
+    }
+    free(tiles);
+    return rc;
+}

@@ -59,6 +59,18 @@ void dwo_circshift(float *A, int64_t M, int64_t N, int64_t P,
 float dwo_idiv(const float *y, const float *g, int64_t M, int64_t N, int64_t P,
                int64_t wM, int64_t wN, int64_t wP);
 
+/* PSF preparation and tiling (dwo.c cites the reference lines). */
+float *dwo_psf_autocrop(float *psf, int64_t *pM, int64_t *pN, int64_t *pP, int64_t M, int64_t N, int64_t P,
+                        int bq, float xycropfactor);
+int dwo_psf_prepare(const float *psf, int64_t pM, int64_t pN, int64_t pP, int64_t M, int64_t N, int64_t P,
+                    int bq, float xycropfactor, float *out, int64_t out_dims[3]);
+int dwo_tiling_create(int64_t M, int64_t N, int64_t P, int64_t max_size, int64_t overlap, int64_t *tiles,
+                      int capacity);
+float dwo_tile_weight(const int64_t *tile, int64_t m, int64_t n);
+int dwo_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, const float *psf, int64_t pM,
+                         int64_t pN, int64_t pP, int64_t tile_size, int64_t overlap, float offset,
+                         float xycropfactor, dwo_opts *s, float *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,7 +79,18 @@ def _lib(kind: str) -> ctypes.CDLL:
     fn.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                    ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                    ctypes.POINTER(DwoOpts), ctypes.c_void_p]
+    i64, vp, f32 = ctypes.c_int64, ctypes.c_void_p, ctypes.c_float
+    tiling = lib.dwo_tiling_create if kind == "port" else lib.dwref_tiling_create
+    tiling.restype = ctypes.c_int
+    tiling.argtypes = [i64] * 5 + [vp, ctypes.c_int]
+    tiled = lib.dwo_deconvolve_tiled if kind == "port" else lib.dwref_deconvolve_tiled
+    tiled.restype = ctypes.c_int
+    tiled.argtypes = [vp, i64, i64, i64, vp, i64, i64, i64, i64, i64, f32, f32, ctypes.POINTER(DwoOpts), vp]
+    if kind == "reference":
+        lib.dwref_tiling_weights.argtypes = [i64] * 5 + [ctypes.c_int, vp, vp]
     if kind == "port":
+        lib.dwo_psf_prepare.restype = ctypes.c_int
+        lib.dwo_psf_prepare.argtypes = [vp] + [i64] * 6 + [ctypes.c_int, f32, vp, ctypes.POINTER(i64)]
         lib.dwo_idiv.restype = ctypes.c_float
         lib.dwo_idiv.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int64] * 6
         lib.dwo_fft_r2c.argtypes = [ctypes.c_void_p] + [ctypes.c_int64] * 3 + [ctypes.c_void_p, ctypes.c_int]
@@ -104,20 +115,13 @@ class Result:
         self.setup_seconds = opts.setup_seconds
 
 
-def deconvolve(im: np.ndarray, psf: np.ndarray, *, method: str = "shb", n_iter: int = 50,
-               iter_type: int = ITER_FIXED, maxiter: int = 250, err_rel: float = 0.02,
-               err_abs: float = 1.0, bg: float | None = None, positivity: bool = True,
-               border_quality: int = 2, start: int = START_FLAT, metric: int = METRIC_IDIV,
-               alphamax: float = 1.0, threads: int = 0, work=None,
-               impl: str = "port") -> Result:
-    """Run the CPU checker on ``im`` (P, N, M) float32 with ``psf`` (pP, pN, pM).
-
-    ``bg=None`` means automatic background (bg_auto).  ``work`` optionally
-    gives a padded job size (Wx, Wy, Wz) for the port (bq=2 only)."""
-    im = np.ascontiguousarray(im, dtype=np.float32)
-    psf = np.ascontiguousarray(psf, dtype=np.float32)
-    P, N, M = im.shape
-    pP, pN, pM = psf.shape
+def make_opts(*, method: str = "shb", n_iter: int = 50, iter_type: int = ITER_FIXED, maxiter: int = 250,
+              err_rel: float = 0.02, err_abs: float = 1.0, bg: float | None = None, positivity: bool = True,
+              border_quality: int = 2, start: int = START_FLAT, metric: int = METRIC_IDIV,
+              alphamax: float = 1.0, threads: int = 0, work=None) -> DwoOpts:
+    """dwo_opts from keyword options; ``bg=None`` means automatic background
+    (bg_auto); ``work`` optionally gives a padded job size (Wx, Wy, Wz) for the
+    port (bq=2 only)."""
     o = DwoOpts()
     o.method = METHOD_SHB if method == "shb" else METHOD_RL
     o.n_iter = n_iter
@@ -135,7 +139,18 @@ def deconvolve(im: np.ndarray, psf: np.ndarray, *, method: str = "shb", n_iter: 
     o.threads = threads if threads > 0 else (os.cpu_count() or 1)
     if work is not None:
         o.work[0], o.work[1], o.work[2] = (int(w) for w in work)
-    cap = max(maxiter, n_iter, 1)
+    return o
+
+
+def deconvolve(im: np.ndarray, psf: np.ndarray, *, impl: str = "port", **kw) -> Result:
+    """Run the CPU checker on ``im`` (P, N, M) float32 with ``psf`` (pP, pN, pM);
+    options as :func:`make_opts`."""
+    im = np.ascontiguousarray(im, dtype=np.float32)
+    psf = np.ascontiguousarray(psf, dtype=np.float32)
+    P, N, M = im.shape
+    pP, pN, pM = psf.shape
+    o = make_opts(**kw)
+    cap = max(o.maxiter, o.n_iter, 1)
     trace = np.zeros(cap, dtype=np.float32)
     o.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     o.trace_capacity = cap
@@ -146,6 +161,59 @@ def deconvolve(im: np.ndarray, psf: np.ndarray, *, method: str = "shb", n_iter: 
     if rc != 0:
         raise RuntimeError(f"oracle ({impl}) rejected the input: code {rc}")
     return Result(out, trace[: o.iterations_done].copy(), o)
+
+
+def psf_prepare(psf: np.ndarray, shape, border_quality: int = 2, xycropfactor: float = 0.001) -> np.ndarray:
+    """dw_run's normalise / psf_autocrop / normalise (oracle/dwo.c)."""
+    p = np.ascontiguousarray(psf, dtype=np.float32)
+    P, N, M = shape
+    pP, pN, pM = p.shape
+    out = np.empty(p.size, dtype=np.float32)
+    dims = (ctypes.c_int64 * 3)()
+    _lib("port").dwo_psf_prepare(p.ctypes.data, pM, pN, pP, M, N, P, border_quality,
+                                 ctypes.c_float(xycropfactor), out.ctypes.data, dims)
+    return out[: dims[0] * dims[1] * dims[2]].reshape(dims[2], dims[1], dims[0]).copy()
+
+
+def tiling_create(shape, max_size: int, overlap: int = 20, impl: str = "port") -> np.ndarray:
+    """Tiles as an (n, 18) int64 array: size[3], pos[6], xpos[6], xsize[3]
+    (x, y, z order); ``impl="reference"`` runs the reference's tiling.c."""
+    P, N, M = shape
+    lib = _lib(impl)
+    fn = lib.dwo_tiling_create if impl == "port" else lib.dwref_tiling_create
+    n = fn(M, N, P, max_size, overlap, None, 0)
+    t = np.zeros((n, 18), dtype=np.int64)
+    fn(M, N, P, max_size, overlap, t.ctypes.data, n)
+    return t
+
+
+def tiling_weights(shape, max_size: int, overlap: int, tid: int):
+    """The reference's tile_getWeight for tile ``tid`` and tiling_getWeights,
+    over the (N, M) plane (tiling.c:169-223)."""
+    P, N, M = shape
+    wt = np.zeros((N, M), np.float32)
+    ws = np.zeros((N, M), np.float32)
+    _lib("reference").dwref_tiling_weights(M, N, P, max_size, overlap, tid, wt.ctypes.data, ws.ctypes.data)
+    return wt, ws
+
+
+def deconvolve_tiled(im: np.ndarray, psf: np.ndarray, tile_size: int, overlap: int = 20, offset: float = 5.0,
+                     xycropfactor: float = 0.001, impl: str = "port", **kw) -> Result:
+    """deconvolve_tiles (dw.c:2001-2229) in memory; ``psf`` as dw_run hands it
+    over; options as :func:`make_opts`."""
+    im = np.ascontiguousarray(im, dtype=np.float32)
+    psf = np.ascontiguousarray(psf, dtype=np.float32)
+    P, N, M = im.shape
+    pP, pN, pM = psf.shape
+    o = make_opts(**kw)
+    out = np.empty_like(im)
+    lib = _lib(impl)
+    fn = lib.dwo_deconvolve_tiled if impl == "port" else lib.dwref_deconvolve_tiled
+    rc = fn(im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP, tile_size, overlap, ctypes.c_float(offset),
+            ctypes.c_float(xycropfactor), ctypes.byref(o), out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle ({impl}) rejected the tiled input: code {rc}")
+    return Result(out, np.zeros(0, np.float32), o)
 
 
 def idiv(y: np.ndarray, g: np.ndarray) -> float:

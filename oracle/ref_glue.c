@@ -2,7 +2,8 @@
  *
  * TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles the reference's
  * src/method_shb.c, src/method_rl.c, src/fft.c, src/fim.c, src/dw_util.c,
- * src/quickselect.c and src/ftab.c unmodified, from where they lie in the
+ * src/quickselect.c, src/ftab.c, src/npio.c and src/tiling.c unmodified, from
+ * where they lie in the
  * reference tree, against oracle/include (FFTW-API shim, libtiff type stub).
  * Those files call a handful of helpers that live in src/dw.c, which pulls in
  * every other deconwolf tool and cannot be compiled here; this file restates
@@ -26,6 +27,7 @@
 #include "fft.h"
 #include "method_shb.h"
 #include "method_rl.h"
+#include "tiling.h"
 #include "dwo.h"
 
 /* ------------------------------------------------ trace of the iterator */
@@ -300,5 +302,103 @@ int dwref_deconvolve(const float *im, int64_t M, int64_t N, int64_t P,
     fim_free(imc);
     fclose(s->log);
     free(s);
+    return rc;
+}
+
+/* ------------------------------------------------ tiling */
+
+float *fim_tiff_read_sub(ftif_t *f, const char *fName, ttags *T, int64_t *M0, int64_t *N0, int64_t *P0, int sub,
+                         int64_t sM, int64_t sN, int64_t sP, int64_t wM, int64_t wN, int64_t wP)
+{
+    (void) f; (void) fName; (void) T; (void) M0; (void) N0; (void) P0; (void) sub;
+    (void) sM; (void) sN; (void) sP; (void) wM; (void) wN; (void) wP;
+    io_unreachable("fim_tiff_read_sub");
+    return NULL;
+}
+
+/* The reference's tiling_create (src/tiling.c:70-130), flattened to 18
+ * int64 per tile (size[3], pos[6], xpos[6], xsize[3]); returns the count. */
+int dwref_tiling_create(int64_t M, int64_t N, int64_t P, int64_t max_size, int64_t overlap, int64_t *tiles,
+                        int capacity)
+{
+    tiling *T = tiling_create(M, N, P, max_size, overlap);
+    int nt = T->nTiles;
+    if (tiles && capacity >= nt)
+        for (int b = 0; b < nt; b++) {
+            tile *t = T->tiles[b];
+            memcpy(tiles + 18 * b, t->size, 3 * sizeof(int64_t));
+            memcpy(tiles + 18 * b + 3, t->pos, 6 * sizeof(int64_t));
+            memcpy(tiles + 18 * b + 9, t->xpos, 6 * sizeof(int64_t));
+            memcpy(tiles + 18 * b + 15, t->xsize, 3 * sizeof(int64_t));
+        }
+    tiling_free(T);
+    free(T);
+    return nt;
+}
+
+/* tiling_getWeights (src/tiling.c:215-223) over a whole M x N plane, for
+ * pinning the blend weights. */
+void dwref_tiling_weights(int64_t M, int64_t N, int64_t P, int64_t max_size, int64_t overlap, int tid,
+                          float *w_tile, float *w_sum)
+{
+    tiling *T = tiling_create(M, N, P, max_size, overlap);
+    for (int64_t n = 0; n < N; n++)
+        for (int64_t m = 0; m < M; m++) {
+            w_tile[m + n * M] = tile_getWeight(T->tiles[tid], m, n, 0);
+            w_sum[m + n * M] = tiling_getWeights(T, m, n, 0);
+        }
+    tiling_free(T);
+    free(T);
+}
+
+/* deconvolve_tiles (src/dw.c:2093-2153) with the reference's tiling_create,
+ * tiling_get_tile, fim_normalize_sum1, fim_add_scalar, fim_project_positive
+ * and tiling_put_tile; psf_autocrop lives in dw.c and is the oracle's
+ * restatement (dwo_psf_autocrop).  The image and result stay in memory
+ * instead of the temporary raw files.  Returns 0, or -3 for one tile. */
+int dwref_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, const float *psf, int64_t pM,
+                           int64_t pN, int64_t pP, int64_t tile_size, int64_t overlap, float offset,
+                           float xycropfactor, dwo_opts *o, float *out)
+{
+    tiling *T = tiling_create(M, N, P, tile_size, overlap);
+    if (T->nTiles == 1) {
+        tiling_free(T);
+        free(T);
+        return -3;
+    }
+    memset(out, 0, sizeof(float) * (size_t) (M * N * P));
+    int rc = 0;
+    for (int tt = 0; tt < T->nTiles && rc == 0; tt++) {
+        float *tpsf = fim_copy(psf, (size_t) (pM * pN * pP));
+        int64_t tpM = pM, tpN = pN, tpP = pP;
+        float *im_tile = tiling_get_tile(T, tt, im);
+        int64_t tileM = T->tiles[tt]->xsize[0], tileN = T->tiles[tt]->xsize[1], tileP = T->tiles[tt]->xsize[2];
+        fim_normalize_sum1(tpsf, tpM, tpN, tpP);
+        float *tp = malloc(sizeof(float) * (size_t) (pM * pN * pP));
+        memcpy(tp, tpsf, sizeof(float) * (size_t) (pM * pN * pP));
+        fim_free(tpsf);
+        tp = dwo_psf_autocrop(tp, &tpM, &tpN, &tpP, tileM, tileN, tileP, o->border_quality, xycropfactor);
+        fim_normalize_sum1(tp, tpM, tpN, tpP);
+        size_t tv = (size_t) (tileM * tileN * tileP);
+        if (offset > 0) fim_add_scalar(im_tile, tv, offset);
+        float *res = fim_malloc(sizeof(float) * tv);
+        dwo_opts so = *o;
+        so.error_trace = NULL;
+        so.trace_capacity = 0;
+        rc = dwref_deconvolve(im_tile, tileM, tileN, tileP, tp, tpM, tpN, tpP, &so, res);
+        o->iterations_done = so.iterations_done;
+        fim_free(im_tile);
+        free(tp);
+        if (rc == 0) {
+            if (offset > 0) {
+                fim_add_scalar(res, tv, -offset);
+                fim_project_positive(res, tv);
+            }
+            tiling_put_tile(T, tt, out, res);
+        }
+        fim_free(res);
+    }
+    tiling_free(T);
+    free(T);
     return rc;
 }
