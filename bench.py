@@ -39,6 +39,7 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "shb-2048x2048x60"
 SMALL = "shb-256x256x40"
+PROFILE_CASE = "shb-1024x1024x20"  # hardware-counter captures (profiles/)
 ITERS = 50
 # generated inputs are cached between runs of one machine (kept out of git and gpurun snapshots)
 CACHE = os.environ.get("DWCU_INPUT_CACHE", os.path.join(ROOT, "_cache"))
@@ -154,33 +155,45 @@ def cpu_baseline_entry(im, psf, crop=384, iters=2):
 
 
 def run_reference_arm(args):
+    """deconwolf's own CPU SHB (oracle/_ref: the reference's method code,
+    FFTW replaced by the oracle FFT) with all host threads, on a bounded crop
+    of the workload: warm-up + timed iterations in one run, the timed ones
+    read from the reference iterator's per-iteration timestamps, scaled per
+    job voxel to the full job (time is linear in job voxels for a fixed PSF)."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
     from deconwolf_b200 import synthetic
-    im, psf = synthetic.config_inputs(WORKLOAD, CACHE)
-    crop = 384 if args.steps + args.warmup <= 12 else 256
+    im, psf = synthetic.config_inputs(args.workload, CACHE)
+    P, N, M = im.shape
+    crop = min(M, N, 384 if args.steps + args.warmup <= 12 else 256)
     from oracle import pyoracle as po
     sub = np.ascontiguousarray(im[:, :crop, :crop])
     impl = "reference" if po.available("reference") else "port"
     n = args.warmup + args.steps
-    # per-iteration times from the reference's own iterator (the glue records them)
     r = po.deconvolve(sub, psf, method="shb", n_iter=n, impl=impl, threads=os.cpu_count())
-    per_it = r.loop_seconds / max(1, r.iterations)
+    if impl == "reference":
+        ts = po.iteration_seconds()
+        per_it = float(np.mean(ts[args.warmup:n])) if len(ts) >= n else r.loop_seconds / max(1, r.iterations)
+    else:
+        per_it = r.loop_seconds / max(1, r.iterations)
     job_crop = full_job_voxels(sub.shape, psf.shape)
     t_full = per_it * full_job_voxels(im.shape, psf.shape) / job_crop
     value = im.size * 1e-6 / t_full
+    sample = (f"{n} SHB iterations ({args.warmup} warm-up, {args.steps} timed) of deconwolf's CPU method code "
+              f"({impl} build, FFTW replaced by the oracle FFT, {os.cpu_count()} threads) on a "
+              f"{crop}x{crop}x{P} crop with the full {psf.shape[2]}x{psf.shape[1]}x{psf.shape[0]} PSF "
+              f"(job {crop + psf.shape[2] - 1}x{crop + psf.shape[1] - 1}x{P + psf.shape[0] - 1}); "
+              f"{per_it:.3f} s/iteration scaled per job voxel to the full job")
     line = {
-        "impl": "reference", "metric": "Mvoxel*iter/s (SHB, 2048x2048x60)", "value": value,
-        "unit": "Mvoxel*iter/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t_full * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "image": [2048, 2048, 60], "psf": [181, 181, 119], "method": "shb",
-                   "iterations_per_step": 1, "crop": [crop, crop, 60]},
+        "impl": "reference", "metric": "Mvoxel*iter/s (SHB, %s)" % args.workload.split("-", 1)[1],
+        "value": value, "unit": "Mvoxel*iter/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_full * ITERS * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Poisson image, Born-Wolf PSF)",
+        "config": {"workload": args.workload, "image": [M, N, P], "psf": list(psf.shape[::-1]), "method": "shb",
+                   "iterations_per_step": ITERS, "crop": [crop, crop, P]},
         "cpu_baseline": {"value": value, "unit": "Mvoxel*iter/s", "cores": os.cpu_count(),
-                         "kind": "reference" if impl == "reference" else "port",
-                         "sample": f"{n} SHB iterations (first {args.warmup} untimed in spirit; mean over all) of "
-                                   f"deconwolf's CPU method code on a {crop}x{crop}x60 crop, extrapolated per job voxel"},
+                         "kind": "reference" if impl == "reference" else "port", "sample": sample},
         "e2e": {"value": value, "unit": "Mvoxel*iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -195,7 +208,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, SMALL])
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, SMALL, PROFILE_CASE])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -320,22 +333,27 @@ def main():
         roof = {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
                 "algorithmic_bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": avg_s * 1e3}
+        # ncu DRAM bytes per launch of this kernel class on the capture case,
+        # scaled to this launch by the algorithmic bytes (units processed)
         prof_path = os.path.join(ROOT, "profiles", "kernel_traffic.json")
         if os.path.exists(prof_path):
-            try:
-                with open(prof_path) as f:
-                    tr = json.load(f).get(WORKLOAD if args.workload == WORKLOAD else args.workload, {})
-                roof["traffic"] = tr.get(dom["name"])
-            except Exception:
-                pass
+            with open(prof_path) as f:
+                tr = json.load(f)
+            k = tr["kernels"].get(dom["name"])
+            if k:
+                roof["traffic"] = k["traffic_over_algorithmic"] * dom["bytes_per_launch"]
+                roof["traffic_source"] = (f"ncu dram__bytes_read.sum + dram__bytes_write.sum on "
+                                          f"{tr['capture']['workload']} ({k['dram_bytes_per_launch']:.4g} B per "
+                                          f"launch), scaled by algorithmic bytes")
     kernels = sorted(
         ({"name": s["name"], "launches": s["launches"], "ms": round(s["ms"], 3),
+          "bytes_per_launch": s["bytes_per_launch"],
           "GBps": round(s["bytes_per_launch"] * s["launches"] / (s["ms"] * 1e-3) / 1e9, 1)} for s in stats),
         key=lambda d: -d["ms"])
     total_k = sum(s["ms"] for s in stats) or 1.0
 
     line = {
-        "metric": "Mvoxel*iter/s (SHB, 2048x2048x60)" if args.workload == WORKLOAD else "Mvoxel*iter/s (SHB, 256x256x40)",
+        "metric": "Mvoxel*iter/s (SHB, %s)" % args.workload.split("-", 1)[1],
         "value": value, "unit": "Mvoxel*iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded Poisson image, Born-Wolf PSF)",

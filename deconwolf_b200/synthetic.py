@@ -74,6 +74,10 @@ CONFIGS = {
     "shb-256x256x40": dict(shape=(40, 256, 256), psf_shape=(79, 127, 127), lam=466.0, K=1500, B=40, bg=100.0, seed=1),
     "shb-2048x2048x60": dict(shape=(60, 2048, 2048), psf_shape=(119, 181, 181), lam=670.0, K=40000, B=600, bg=100.0,
                              seed=2),
+    # a mid-size case of the same kernels (per-voxel work as above, device
+    # buffers > L2, a few GB on the device): used for hardware-counter captures
+    "shb-1024x1024x20": dict(shape=(20, 1024, 1024), psf_shape=(39, 181, 181), lam=670.0, K=3300, B=50, bg=100.0,
+                             seed=3),
 }
 
 

@@ -12,7 +12,7 @@
  * the iteration honours are carried in dwcu_opts, the result goes to a caller
  * buffer, and failures return a status instead of exit().  The reference-side
  * glue that adapts dw_opts and registers deconvolve_shb_cu / deconvolve_rl_cu
- * as dw_functions is shown in INTEGRATION.md.
+ * as dw_functions is deconwolf_b200/glue/method_shb_cu.c.
  *
  * Layout everywhere: float32, x fastest, index = m + n*M + p*M*N (deconwolf's
  * fim layout), no row padding at this boundary.

@@ -87,6 +87,8 @@ def _lib(kind: str) -> ctypes.CDLL:
     tiled.restype = ctypes.c_int
     tiled.argtypes = [vp, i64, i64, i64, vp, i64, i64, i64, i64, i64, f32, f32, ctypes.POINTER(DwoOpts), vp]
     if kind == "reference":
+        lib.dwref_iteration_seconds.restype = ctypes.c_int
+        lib.dwref_iteration_seconds.argtypes = [vp, ctypes.c_int]
         lib.dwref_tiling_weights.argtypes = [i64] * 5 + [ctypes.c_int, vp, vp]
     if kind == "port":
         lib.dwo_psf_prepare.restype = ctypes.c_int
@@ -214,6 +216,14 @@ def deconvolve_tiled(im: np.ndarray, psf: np.ndarray, tile_size: int, overlap: i
     if rc != 0:
         raise RuntimeError(f"oracle ({impl}) rejected the tiled input: code {rc}")
     return Result(out, np.zeros(0, np.float32), o)
+
+
+def iteration_seconds() -> np.ndarray:
+    """Per-iteration wall seconds of the last reference run (its iterator's
+    timestamps)."""
+    buf = np.zeros(4096, np.float64)
+    n = _lib("reference").dwref_iteration_seconds(buf.ctypes.data, len(buf))
+    return buf[:n].copy()
 
 
 def idiv(y: np.ndarray, g: np.ndarray) -> float:

@@ -35,6 +35,8 @@ static float *g_trace;
 static int g_trace_cap;
 static int g_iters;
 static double g_t_first_next, g_t_last_set;
+#define DWREF_MAX_TIMES 4096
+static double g_t_set[DWREF_MAX_TIMES]; /* end time of each iteration */
 
 static double mono(void)
 {
@@ -86,6 +88,17 @@ void dw_iterator_set_error(dw_iterator_t *it, float err)
     if (g_trace && it->iter >= 0 && it->iter < g_trace_cap) g_trace[it->iter] = err;
     g_iters = it->iter + 1;
     g_t_last_set = mono();
+    if (it->iter >= 0 && it->iter < DWREF_MAX_TIMES) g_t_set[it->iter] = g_t_last_set;
+}
+
+/* Seconds of each iteration of the last dwref_deconvolve call (the first
+ * measured from the loop's first dw_iterator_next); returns the count. */
+int dwref_iteration_seconds(double *out, int cap)
+{
+    int n = g_iters < cap ? g_iters : cap;
+    if (n > DWREF_MAX_TIMES) n = DWREF_MAX_TIMES;
+    for (int k = 0; k < n; k++) out[k] = g_t_set[k] - (k == 0 ? g_t_first_next : g_t_set[k - 1]);
+    return n;
 }
 
 void dw_iterator_show(dw_iterator_t *it, const dw_opts *s) { (void) it; (void) s; }
