@@ -112,7 +112,7 @@ EXPORTS = [
     "dwcu_job_destroy", "dwcu_job_set_stream", "dwcu_job_bytes", "dwcu_last_error",
     "dwcu_abi_version", "dwcu_device_count", "dwcu_launch_count", "dwcu_fft_r2c", "dwcu_fft_c2r",
     "dwcu_profile_enable", "dwcu_profile_collect", "dwcu_batch_run", "dwcu_psf_prepare",
-    "dwcu_tiling_create", "dwcu_deconvolve_tiled",
+    "dwcu_tiling_create", "dwcu_deconvolve_tiled", "dwcu_fft_r2c_noalloc",
 ]
 
 _lib = None
@@ -162,7 +162,7 @@ def lib() -> ctypes.CDLL:
     L.dwcu_profile_enable.restype = ctypes.c_int
     L.dwcu_profile_collect.argtypes = [ctypes.POINTER(KernelStat), i32, ctypes.POINTER(i32)]
     L.dwcu_profile_collect.restype = ctypes.c_int
-    for fn in (L.dwcu_fft_r2c, L.dwcu_fft_c2r):
+    for fn in (L.dwcu_fft_r2c, L.dwcu_fft_c2r, L.dwcu_fft_r2c_noalloc):
         fn.argtypes = [vp, i64, i64, i64, vp, i32, vp]
         fn.restype = ctypes.c_int
     L.dwcu_batch_run.argtypes = [ctypes.POINTER(vp), i32, vp]
@@ -264,6 +264,14 @@ def fft_r2c_device(d_in: int, shape, d_out: int, device: int = 0, stream: int = 
     P, N, M = shape
     _check(lib().dwcu_fft_r2c(ctypes.c_void_p(d_in), M, N, P, ctypes.c_void_p(d_out), device,
                               ctypes.c_void_p(stream or None)))
+
+
+def fft_r2c_noalloc_device(d_in: int, shape, d_out: int, device: int = 0, stream: int = 0) -> None:
+    """:func:`fft_r2c_device` with the library's fixed work space (no device
+    allocation; sizes up to the work space only)."""
+    P, N, M = shape
+    _check(lib().dwcu_fft_r2c_noalloc(ctypes.c_void_p(d_in), M, N, P, ctypes.c_void_p(d_out), device,
+                                      ctypes.c_void_p(stream or None)))
 
 
 def fft_c2r_device(d_in: int, shape, d_out: int, device: int = 0, stream: int = 0) -> None:

@@ -1260,6 +1260,77 @@ static int fft3d(const float *d_in, long long M, long long N, long long P, float
     return DWCU_SUCCESS;
 }
 
+// ---- the R2C transform of fft3d on caller-provided device memory (used by
+// noalloc.cu): sizes of the pieces it needs, then the transform itself
+int fft3d_scratch_sizes(long long M, long long N, long long P, size_t *spec_bytes, size_t *real_bytes)
+{
+    if (M < 2 || N < 1 || P < 1 || (M % 2)) return fail(DWCU_ERROR_INVALID_VALUE, "M must be even and >= 2");
+    if (!find_x((int) (M / 2)) || (N > 1 && !find_lines((int) N)) || !find_lines((int) P))
+        return fail(DWCU_ERROR_UNSUPPORTED, "unsupported transform size %lld x %lld x %lld", M, N, P);
+    const long long XP = (M + 3) & ~3LL, NKB = (M / 2 + 1 + KB - 1) / KB;
+    *spec_bytes = align256(sizeof(float2) * (size_t) (NKB * N * KB * P + 8 * KB));
+    *real_bytes = align256(sizeof(float) * (size_t) (XP * N * P + XP));
+    return DWCU_SUCCESS;
+}
+
+static_assert(sizeof(JobScalars) <= 256, "noalloc.cu reserves 256 bytes for the scalars");
+
+// S (spec_bytes), real (real_bytes) and sc must be zero on entry; tw holds
+// the twiddle tables of the lengths M, M/2, N, P.  Enqueues on `stream`,
+// waits for it and reports a bounded-wait timeout of any pass.
+int fft3d_r2c_scratch(const float *d_in, long long M, long long N, long long P, float *d_out, cudaStream_t stream,
+                      float2 *S, float *real, JobScalars *sc, const float2 *const tw[4])
+{
+    dwcu_job jj;
+    dwcu_job *j = &jj;
+    Geometry &g = j->g;
+    g.M = M; g.N = N; g.P = P; g.pM = g.pN = g.pP = 1;
+    g.wM = g.X = M; g.wN = g.Y = N; g.wP = g.Z = P;
+    g.xp = find_x((int) (M / 2));
+    g.yp = N > 1 ? find_lines((int) N) : nullptr;
+    g.zp = find_lines((int) P);
+    g.ytp = N > 1 ? find_y((int) N) : nullptr;
+    if (!g.xp || (N > 1 && !g.yp) || !g.zp)
+        return fail(DWCU_ERROR_UNSUPPORTED, "unsupported transform size %lld x %lld x %lld", M, N, P);
+    g.XP = (M + 3) & ~3LL;
+    g.NKB = (M / 2 + 1 + KB - 1) / KB;
+    g.GP = (M + 3) & ~3LL;
+    j->s.metric = DWCU_METRIC_IDIV;
+    j->s.positivity = 1;
+    j->stream = stream;
+    j->nxb = x_blocks(g);
+    j->tw_x = tw[0];
+    j->tw_l = tw[1];
+    j->tw_y = tw[2];
+    j->tw_z = tw[3];
+    j->S = S;
+    j->sc = sc;
+    const long long H = M / 2 + 1;
+    const long long nspec = H * N * P;
+    const int fb = (int) std::min<long long>(148 * 16, (nspec + 255) / 256);
+    int rc = DWCU_SUCCESS;
+    if (cudaMemcpy2DAsync(real, sizeof(float) * g.XP, d_in, sizeof(float) * M, sizeof(float) * M, N * P,
+                          cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+        rc = fail(DWCU_ERROR_CUDA, "copy failed");
+    if (rc == DWCU_SUCCESS) rc = pass_x(j, XOP_FWD_COPY, 1, j->S, real, nullptr, nullptr, 0, 0);
+    if (rc == DWCU_SUCCESS) rc = pass_y(j, LINES_FWD, j->S);
+    if (rc == DWCU_SUCCESS) rc = pass_z(j, LINES_FWD, j->S);
+    if (rc == DWCU_SUCCESS) {
+        k_spec_unpack<<<fb, 256, 0, stream>>>(j->S, (int) H, (int) N, (int) P, (int) g.NKB,
+                                               reinterpret_cast<float2 *>(d_out));
+        ++g_launches;
+        if (cudaGetLastError() != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "unpack launch failed");
+    }
+    cudaError_t e = cudaStreamSynchronize(stream);
+    JobScalars hs{};
+    if (e == cudaSuccess) e = cudaMemcpy(&hs, sc, sizeof hs, cudaMemcpyDeviceToHost);
+    j->stream = nullptr;
+    if (rc != DWCU_SUCCESS) return rc;
+    if (e != cudaSuccess) return fail(DWCU_ERROR_CUDA, "transform failed: %s", cudaGetErrorString(e));
+    if (hs.flags & ~3) return fail(DWCU_ERROR_TIMEOUT, "a bounded wait in a pass gave up (flags 0x%x)", hs.flags);
+    return DWCU_SUCCESS;
+}
+
 }  // namespace dwcu
 
 // ================================================================ C ABI

@@ -210,6 +210,21 @@ int dwcu_fft_r2c(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_ou
 int dwcu_fft_c2r(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_out, int32_t device,
                  void *stream);
 
+/* dwcu_fft_r2c without any device-memory allocation.  No counterpart in the
+ * reference (deconwolf's fft.c has no allocation-free transform).  Same
+ * transform, arguments and result as dwcu_fft_r2c, but the work space is a
+ * fixed 32 MiB array in the library's device image (one per device) instead
+ * of a cudaMalloc / cudaFree per call: for callers that cannot allocate
+ * (a fixed device-memory budget held by their own pool) or cannot afford the
+ * device-wide synchronisation of cudaFree while other streams of the GPU are
+ * busy.  Transforms whose spectrum, staged input and twiddle tables need more
+ * than the work space are rejected with DWCU_ERROR_INVALID_VALUE.  The first
+ * call on a device does one-time setup (symbol lookup, kernel attributes).
+ * Calls on one device share the work space: they are serialised by a lock
+ * and each returns after its stream has drained. */
+int dwcu_fft_r2c_noalloc(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_out, int32_t device,
+                         void *stream);
+
 /* ---------------------------------------------------------------- timing */
 
 /* Per-kernel-class timing.  While enabled, every pass the engine launches
