@@ -476,8 +476,10 @@ static int trace_cap(const dwcu_opts &s) { return std::max(1, std::max(s.n_iter,
 
 static int launch_lines(dwcu_job *j, const LinesPlan *p, const float2 *tw, long long n, long long line_stride,
                         long long outer_stride, long long nouter, long long ncols, int mode, float2 *data,
-                        const char *axis)
+                        const char *axis, long long nin = -1, long long nout = -1)
 {
+    if (nin < 0) nin = n;
+    if (nout < 0) nout = n;
     if (!p) return DWCU_SUCCESS;  // length-1 axis: identity
     LinesArgs a;
     a.data = data;
@@ -488,48 +490,56 @@ static int launch_lines(dwcu_job *j, const LinesPlan *p, const float2 *tw, long 
     a.ncols = (int) ncols;
     a.ntiles = (int) ((ncols + p->T - 1) / p->T);
     a.mode = mode;
+    a.nin = (int) nin;
+    a.nout = (int) nout;
     long long nb = (long long) a.ntiles * nouter;
     if (nb > 0x7fffffffLL) return fail(DWCU_ERROR_UNSUPPORTED, "grid too large");
     static const char *names[] = {"lines_fwd", "lines_inv", "lines_conv", "lines_conv_conj"};
     char nm[40];
     snprintf(nm, sizeof nm, "%s_%s", names[mode], axis);
-    const double elems = (double) ncols * (double) nouter * (double) n;
-    ProfScope ps(nm, elems * 8.0 * (mode >= LINES_CONV ? 3.0 : 2.0), j->stream);
+    // algorithmic bytes: the elements read, the OTF (convolve modes), the elements written
+    const double lines = (double) ncols * (double) nouter;
+    const double bytes = 8.0 * lines * ((double) nin + (double) nout + (mode >= LINES_CONV ? (double) n : 0.0));
+    ProfScope ps(nm, bytes, j->stream);
     p->launch(a, (int) nb, j->stream);
     CHECK_LAUNCH();
     return DWCU_SUCCESS;
 }
 
-static int pass_y(dwcu_job *j, int mode, float2 *data)
+// y transforms of the planes z < planes (default: all)
+static int pass_y(dwcu_job *j, int mode, float2 *data, long long planes = -1)
 {
     const Geometry &g = j->g;
     if (g.Y == 1) return DWCU_SUCCESS;
+    if (planes < 0) planes = g.Z;
     if (g.ytp) {
         // one contiguous tile per (z, kx block): 4 lines of Y elements
         YArgs a;
         a.data = data;
         a.tw = j->tw_y;
         a.err = &j->sc->flags;
-        a.ntiles = (int) (g.Z * g.NKB);
+        a.ntiles = (int) (planes * g.NKB);
         a.dir = (mode == LINES_INV) ? +1 : -1;
-        ProfScope ps(mode == LINES_INV ? "y_inv" : "y_fwd", 16.0 * (double) g.spec_elems(), j->stream);
+        ProfScope ps(mode == LINES_INV ? "y_inv" : "y_fwd", 16.0 * (double) g.NKB * KB * g.Y * planes, j->stream);
         g.ytp->launch(a, j->stream);
         CHECK_LAUNCH();
         return DWCU_SUCCESS;
     }
     // lines along y: 4 contiguous columns, stride KB, outer = (z, kx block)
-    return launch_lines(j, g.yp, j->tw_y, g.Y, KB, g.Y * KB, g.Z * g.NKB, KB, mode, data, "y");
+    return launch_lines(j, g.yp, j->tw_y, g.Y, KB, g.Y * KB, planes * g.NKB, KB, mode, data, "y");
 }
-static int pass_z(dwcu_job *j, int mode, float2 *data)
+// z transforms; planes >= nin are taken as zero and not read, only planes
+// < nout are written (defaults: all)
+static int pass_z(dwcu_job *j, int mode, float2 *data, long long nin = -1, long long nout = -1)
 {
     const Geometry &g = j->g;
     // lines along z: every (kx block, y, kx) of a plane is a column; stride = plane
     const long long plane = g.NKB * g.Y * KB;
-    return launch_lines(j, g.zp, j->tw_z, g.Z, plane, 0, 1, plane, mode, data, "z");
+    return launch_lines(j, g.zp, j->tw_z, g.Z, plane, 0, 1, plane, mode, data, "z", nin, nout);
 }
 
 static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, const float *srcp, float *dst,
-                  double alpha, double alpha_next)
+                  double alpha, double alpha_next, long long tiles = -1)
 {
     const Geometry &g = j->g;
     XArgs a;
@@ -547,7 +557,7 @@ static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, con
     a.X = g.XP;
     a.GP = g.GP;
     a.nkb = (int) g.NKB;
-    a.ntiles = (int) j->nxb;
+    a.ntiles = (int) (tiles < 0 ? j->nxb : tiles);
     a.Y = (int) g.Y;
     a.Z = (int) g.Z;
     a.M = (int) g.M;
@@ -571,17 +581,25 @@ static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, con
     double bytes = (op >= XOP_RATIO_SHB ? C : 0.0) + (r2c ? C : 0.0) + (real_in[op] + real_out[op]) * R;
     if (op == XOP_UPDATE_SHB && !j->W) bytes -= R;
     if (op == XOP_UPDATE_RL && !j->W) bytes -= R;
-    if (op == XOP_RATIO_SHB || op == XOP_RATIO_RL || op == XOP_ERROR_ONLY) bytes += G;
+    if (op == XOP_RATIO_SHB || op == XOP_RATIO_RL || op == XOP_ERROR_ONLY) {
+        // only tiles holding image rows read their spectrum rows; the
+        // launched tiles write theirs
+        const long long Rr = g.xp->R, ytiles = (g.Y + Rr - 1) / Rr;
+        const double rows_img = (double) g.P * (double) std::min(g.Y, ((g.N + Rr - 1) / Rr) * Rr);
+        const double rows = (double) g.Y * (double) g.Z;
+        const double launched = (double) std::min(rows, (double) a.ntiles / (double) ytiles * (double) g.Y);
+        bytes = C * rows_img / rows + (r2c ? C * launched / rows : 0.0) + G;
+    }
     ProfScope ps(names[op], bytes, j->stream);
     g.xp->launch(a, j->stream);
     CHECK_LAUNCH();
     return DWCU_SUCCESS;
 }
 
-static int err_final(dwcu_job *j, int k)
+static int err_final(dwcu_job *j, int k, long long tiles)
 {
     const Geometry &g = j->g;
-    k_err_final<<<1, kRedThreads, 0, j->stream>>>(j->partial, (int) j->nxb, (double) (g.M * g.N * g.P), j->err + k);
+    k_err_final<<<1, kRedThreads, 0, j->stream>>>(j->partial, (int) tiles, (double) (g.M * g.N * g.P), j->err + k);
     CHECK_LAUNCH();
     return DWCU_SUCCESS;
 }
@@ -609,15 +627,44 @@ static int conv(dwcu_job *j, int conj)
     return DWCU_SUCCESS;
 }
 
+// The iteration's convolutions, pruned to the planes that matter.  The
+// forward one (y = K p) is only read on the image (z < P): its z pass writes
+// planes z < P and its inverse y pass transforms only those.  The ratio that
+// the back-projection transforms is zero outside the image for SHB
+// (method_shb.c:44-46), so its planes z >= P are zero: the forward y pass
+// skips them and the z pass reads them as zero.  (RL's ratio is 1e-6 there,
+// so its back-projection stays complete.)
+static int conv_forward(dwcu_job *j)
+{
+    const Geometry &g = j->g;
+    TRY(pass_y(j, LINES_FWD, j->S));
+    TRY(pass_z(j, LINES_CONV, j->S, g.Z, g.P));
+    TRY(pass_y(j, LINES_INV, j->S, g.P));
+    return DWCU_SUCCESS;
+}
+static int conv_backward(dwcu_job *j)
+{
+    const Geometry &g = j->g;
+    if (j->s.method != DWCU_METHOD_SHB) return conv(j, 1);
+    TRY(pass_y(j, LINES_FWD, j->S, g.P));
+    TRY(pass_z(j, LINES_CONV_CONJ, j->S, g.P, g.Z));
+    TRY(pass_y(j, LINES_INV, j->S));
+    return DWCU_SUCCESS;
+}
+
 // forward half of iteration k: y = K p_k, error_k; when `ratio`, also the
-// ratio's transform into S
+// ratio's transform into S.  The x pass runs the tiles of planes z < P only
+// when nothing reads the other planes (SHB, or the error alone).
 static int iter_forward(dwcu_job *j, int k, bool ratio)
 {
+    const Geometry &g = j->g;
     const bool shb = (j->s.method == DWCU_METHOD_SHB);
-    TRY(conv(j, 0));
+    TRY(conv_forward(j));
     int op = ratio ? (shb ? XOP_RATIO_SHB : XOP_RATIO_RL) : XOP_ERROR_ONLY;
-    TRY(pass_x(j, op, ratio ? 1 : 0, j->S, nullptr, nullptr, nullptr, 0, 0));
-    TRY(err_final(j, k));
+    const long long ytiles = (g.Y + g.xp->R - 1) / g.xp->R;
+    const long long tiles = (op == XOP_RATIO_RL) ? j->nxb : g.P * ytiles;
+    TRY(pass_x(j, op, ratio ? 1 : 0, j->S, nullptr, nullptr, nullptr, 0, 0, tiles));
+    TRY(err_final(j, k, tiles));
     return DWCU_SUCCESS;
 }
 
@@ -626,7 +673,7 @@ static int iter_forward(dwcu_job *j, int k, bool ratio)
 static int iter_backward(dwcu_job *j, int k, bool next)
 {
     const bool shb = (j->s.method == DWCU_METHOD_SHB);
-    TRY(conv(j, 1));
+    TRY(conv_backward(j));
     if (shb) {
         TRY(pass_x(j, XOP_UPDATE_SHB, next ? 1 : 0, j->S, j->xa, j->xb, j->xb, shb_alpha(k, j->s.alphamax),
                    shb_alpha(k + 1, j->s.alphamax)));

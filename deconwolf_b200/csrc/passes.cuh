@@ -171,6 +171,8 @@ struct LinesArgs {
     int ncols;               // adjacent lines (contiguous columns) per outer block
     int ntiles;              // ceil(ncols / T)
     int mode;
+    int nin;                 // elements [0, nin) of a line are read; the rest are zero
+    int nout;                // elements [0, nout) of a line are written
 };
 
 template <class RD, int T>
@@ -205,8 +207,10 @@ k_lines(LinesArgs a)
     float2 v[1][RD::RA];
     if (t < N / RD::RA) {
 #pragma unroll
-        for (int r = 0; r < RD::RA; ++r)
-            v[0][r] = valid ? base[(long long) (t + r * (N / RD::RA)) * ls] : make_float2(0.f, 0.f);
+        for (int r = 0; r < RD::RA; ++r) {
+            const int n = t + r * (N / RD::RA);
+            v[0][r] = (valid && n < a.nin) ? base[(long long) n * ls] : make_float2(0.f, 0.f);
+        }
     }
     float2 o[1][RD::RL];
     if (mode == LINES_INV)
@@ -217,7 +221,8 @@ k_lines(LinesArgs a)
     if (mode == LINES_FWD || mode == LINES_INV) {
         if (t < SL && valid) {
 #pragma unroll
-            for (int r = 0; r < RD::RL; ++r) base[(long long) (t + r * SL) * ls] = o[0][r];
+            for (int r = 0; r < RD::RL; ++r)
+                if (t + r * SL < a.nout) base[(long long) (t + r * SL) * ls] = o[0][r];
         }
         return;
     }
@@ -236,7 +241,8 @@ k_lines(LinesArgs a)
     constexpr int SQ = N / RV::RL;
     if (t < SQ && valid) {
 #pragma unroll
-        for (int r = 0; r < RV::RL; ++r) base[(long long) (t + r * SQ) * ls] = q[0][r];
+        for (int r = 0; r < RV::RL; ++r)
+            if (t + r * SQ < a.nout) base[(long long) (t + r * SQ) * ls] = q[0][r];
     }
 }
 
@@ -666,6 +672,30 @@ k_xpass(XArgs a)
     const int tile = blockIdx.x;
     const int z = tile / ytiles;
     const int y0 = (tile - z * ytiles) * R;
+
+    if constexpr (FAM == XFAM_RATIO) {
+        if (z >= a.P || y0 >= a.N) {
+            // No image row in this tile: the ratio is the same constant on
+            // every row (0 for SHB, method_shb.c:44-46; 1e-6 for RL,
+            // method_rl.c:62-64) and the rows add nothing to the error, so
+            // neither transform is needed: the rows' spectra are c*X at kx = 0
+            // and 0 elsewhere.
+            if (tid == 0) a.partial[tile] = 0.0;
+            if (a.r2c) {
+                const float dc = (op == XOP_RATIO_RL) ? 1e-6f * (float) C::X : 0.f;
+                float2 *Sz = a.S + (long long) z * plane + (long long) y0 * KB;
+                for (int e = tid; e < C::NKB * R * KB; e += C::THREADS) {
+                    const int ki = e % KB;
+                    const int r2 = (e / KB) % R;
+                    const int kb = e / (KB * R);
+                    const int k = kb * KB + ki;
+                    if (k > L || y0 + r2 >= a.Y) continue;
+                    Sz[(long long) kb * a.Y * KB + r2 * KB + ki] = make_float2(k == 0 ? dc : 0.f, 0.f);
+                }
+            }
+            return;
+        }
+    }
 
     // ---- bulk copies of this tile (warp 0)
     const bool grow = rg && z < a.P && y0 < a.N;
