@@ -200,6 +200,172 @@ def run_reference_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------- batched / served workloads
+#
+# Each prints one JSON line: the batched (or served) throughput as `value`,
+# the plain one-job-at-a-time GPU path on the same inputs as `sequential`.
+# Wall-clock timing around host-buffer calls (uploads and downloads inside).
+
+def _common_line(metric, value, args, config, extra):
+    line = {"metric": metric, "value": value, "unit": "Mvoxel*iter/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded Poisson images, Born-Wolf PSFs)", "config": config}
+    line.update(extra)
+    return line
+
+
+def run_tiles(args):
+    import deconwolf_b200 as dw
+    from deconwolf_b200 import synthetic
+    t0 = time.time()
+    im, psf = synthetic.tiled_inputs(CACHE)
+    log(f"inputs {im.shape} in {time.time() - t0:.1f}s")
+    pp = dw.psf_prepare(psf, im.shape)
+    tiles = dw.tiling_create(im.shape, args.tilesize, 50)
+
+    def step(budget=0.0):
+        return dw.deconvolve_tiled(im, pp, args.tilesize, 50, method="shb", n_iter=ITERS, hbm_budget=budget)
+
+    for _ in range(args.warmup):
+        step()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        res = step()
+    dt = (time.perf_counter() - t) / args.steps
+    t = time.perf_counter()
+    seq = step(1.0)  # one tile per batch: the tiles one after another
+    dt_seq = time.perf_counter() - t
+    vox_it = float(im.size) * ITERS
+    P, N, M = im.shape
+    print(json.dumps(_common_line(
+        f"Mvoxel*iter/s (SHB, tiled {M}x{N}x{P})", vox_it / dt / 1e6, args,
+        {"workload": "tiles-4096x4096x60", "image": [M, N, P], "psf": list(psf.shape[::-1]),
+         "tilesize": args.tilesize, "overlap": 50, "tiles": len(tiles), "iterations": ITERS, "method": "shb"},
+        {"ms_per_step": dt * 1e3,
+         "sequential": {"value": vox_it / dt_seq / 1e6, "ms_per_step": dt_seq * 1e3,
+                        "how": "dwcu_deconvolve_tiled with one tile per batch"},
+         "batched_equals_sequential": bool(np.array_equal(res.out, seq.out))})), flush=True)
+    return 0
+
+
+def run_channels(args):
+    import deconwolf_b200 as dw
+    from deconwolf_b200 import synthetic
+    t0 = time.time()
+    chans = []
+    for c in range(6):
+        im, psf = synthetic.channel_inputs(c, CACHE)
+        sp = synthetic.channel_spec(c)
+        chans.append((im, dw.psf_prepare(psf, im.shape), sp["iters"]))
+    log(f"6 channels in {time.time() - t0:.1f}s: " + ", ".join(str(c[0].shape) for c in chans))
+
+    def batched():
+        jobs = []
+        for im, p, it in chans:
+            j = dw.Job(im.shape, p.shape, method="shb", n_iter=it)
+            j.setup(im, p)
+            jobs.append(j)
+        dw.batch_run(jobs)
+        outs = [j.result() for j in jobs]
+        for j in jobs:
+            j.close()
+        return outs
+
+    def sequential():
+        return [dw.run_method(im, p, method="shb", n_iter=it) for im, p, it in chans]
+
+    for _ in range(args.warmup):
+        batched()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        outs = batched()
+    dt = (time.perf_counter() - t) / args.steps
+    sequential()
+    t = time.perf_counter()
+    souts = sequential()
+    dt_seq = time.perf_counter() - t
+    vox_it = float(sum(im.size * it for im, _, it in chans))
+    same = all(np.array_equal(a.out, b.out) for a, b in zip(outs, souts))
+    print(json.dumps(_common_line(
+        "Mvoxel*iter/s (SHB, 6-channel field of view)", vox_it / dt / 1e6, args,
+        {"workload": "channels-6", "channels": [{"image": list(im.shape[::-1]), "psf": list(p.shape[::-1]),
+                                                 "iterations": it} for im, p, it in chans], "method": "shb"},
+        {"ms_per_step": dt * 1e3,
+         "sequential": {"value": vox_it / dt_seq / 1e6, "ms_per_step": dt_seq * 1e3,
+                        "how": "dwcu_deconvolve per channel, one after another"},
+         "batched_equals_sequential": bool(same)})), flush=True)
+    return 0
+
+
+def run_serve(args):
+    import deconwolf_b200 as dw
+    from deconwolf_b200 import synthetic
+    t0 = time.time()
+    reqs = synthetic.serve_requests(args.requests)
+    pool = {}
+    psfs = {}
+    for i, r in enumerate(reqs):
+        key = (r["size"], i % 2)
+        if key not in pool:
+            pool[key] = synthetic.serve_image(*key, cache_dir=CACHE)[0]
+        r["image"] = key
+        if (r["size"], r["lam"]) not in psfs:
+            psfs[(r["size"], r["lam"])] = synthetic.serve_psf(r["size"], r["lam"], CACHE)
+    log(f"{len(reqs)} requests, {len(pool)} images, {len(psfs)} PSFs in {time.time() - t0:.1f}s")
+
+    def inputs(r):
+        return pool[r["image"]], psfs[(r["size"], r["lam"])]
+
+    # served: a submitter thread replays the arrivals
+    sv = dw.Server(hbm_budget=args.hbm_budget, max_active=8, iters_per_turn=8)
+    ids = [None] * len(reqs)
+    start = time.perf_counter()
+
+    def submitter():
+        for i, r in enumerate(reqs):
+            delay = start + r["arrival"] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            im, psf = inputs(r)
+            ids[i] = sv.submit(im, psf, method=r["method"], n_iter=r["iters"])
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    served = [sv.wait(i) for i in ids]
+    st = sv.stats()
+    sv.close()
+    vox_it = float(sum(pool[r["image"]].size * r["iters"] for r in reqs))
+    # sequential: one request at a time, each starting at its arrival or when the previous ends
+    lat = []
+    start = time.perf_counter()
+    seq = []
+    for r in reqs:
+        delay = start + r["arrival"] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        im, psf = inputs(r)
+        seq.append(dw.run_method(im, psf, method=r["method"], n_iter=r["iters"]))
+        lat.append(time.perf_counter() - (start + r["arrival"]))
+    wall_seq = time.perf_counter() - start
+    lat = np.sort(np.array(lat))
+    same = sum(int(np.array_equal(a.out, b.out)) for a, b in zip(served, seq))
+    sizes = [list(s[::-1]) for s in synthetic.SERVE_SIZES]
+    print(json.dumps(_common_line(
+        "Mvoxel*iter/s (SHB/RL serving stream)", st["voxel_iterations"] / st["wall_s"] / 1e6, args,
+        {"workload": "serve-stream", "requests": len(reqs), "arrival_rate_per_s": 2.0, "sizes": sizes,
+         "psf": "181x181x(2P-1) Born-Wolf at the request's wavelength", "iterations": "uniform 20-200",
+         "methods": "SHB/RL 50/50", "hbm_budget_bytes": args.hbm_budget, "max_active": 8, "iters_per_turn": 8},
+        {"latency_p50_s": st["latency_p50_s"], "latency_p99_s": st["latency_p99_s"],
+         "latency_mean_s": st["latency_mean_s"], "wall_s": st["wall_s"],
+         "sequential": {"value": vox_it / wall_seq / 1e6, "wall_s": wall_seq,
+                        "latency_p50_s": float(lat[int(np.ceil(0.5 * len(lat))) - 1]),
+                        "latency_p99_s": float(lat[int(np.ceil(0.99 * len(lat))) - 1]),
+                        "how": "dwcu_deconvolve per request in arrival order"},
+         "served_equals_sequential": f"{same}/{len(reqs)}"})), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- B200 arm
 
 def main():
@@ -208,7 +374,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, SMALL, PROFILE_CASE])
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=[WORKLOAD, SMALL, PROFILE_CASE, "tiles-4096x4096x60", "channels-6", "serve-stream"])
+    ap.add_argument("--tilesize", type=int, default=1024)
+    ap.add_argument("--requests", type=int, default=60, help="serve-stream: number of requests (full stream: 500)")
+    ap.add_argument("--hbm-budget", type=float, default=160e9, help="serve-stream: device bytes for admitted jobs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -217,6 +387,12 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "tiles-4096x4096x60":
+        return run_tiles(args)
+    if args.workload == "channels-6":
+        return run_channels(args)
+    if args.workload == "serve-stream":
+        return run_serve(args)
 
     import torch
     import torch.distributed as dist

@@ -105,6 +105,15 @@ class Tile(ctypes.Structure):
                 ("xpos", ctypes.c_int64 * 6), ("xsize", ctypes.c_int64 * 3)]
 
 
+class ServerStats(ctypes.Structure):
+    """dwcu_server_stats."""
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("cancelled", ctypes.c_int64), ("active", ctypes.c_int64), ("queued", ctypes.c_int64),
+                ("device_bytes_in_use", ctypes.c_double), ("latency_p50_s", ctypes.c_double),
+                ("latency_p99_s", ctypes.c_double), ("latency_mean_s", ctypes.c_double),
+                ("voxel_iterations", ctypes.c_double), ("wall_s", ctypes.c_double)]
+
+
 # every symbol include/dwcu.h declares
 EXPORTS = [
     "dwcu_opts_init", "dwcu_deconvolve", "dwcu_deconvolve_device", "dwcu_plan_size",
@@ -112,7 +121,9 @@ EXPORTS = [
     "dwcu_job_destroy", "dwcu_job_set_stream", "dwcu_job_bytes", "dwcu_last_error",
     "dwcu_abi_version", "dwcu_device_count", "dwcu_launch_count", "dwcu_fft_r2c", "dwcu_fft_c2r",
     "dwcu_profile_enable", "dwcu_profile_collect", "dwcu_batch_run", "dwcu_psf_prepare",
-    "dwcu_tiling_create", "dwcu_deconvolve_tiled", "dwcu_fft_r2c_noalloc",
+    "dwcu_tiling_create", "dwcu_deconvolve_tiled", "dwcu_fft_r2c_noalloc", "dwcu_server_create",
+    "dwcu_server_submit", "dwcu_server_wait", "dwcu_server_cancel", "dwcu_server_get_stats",
+    "dwcu_server_destroy",
 ]
 
 _lib = None
@@ -165,6 +176,18 @@ def lib() -> ctypes.CDLL:
     for fn in (L.dwcu_fft_r2c, L.dwcu_fft_c2r, L.dwcu_fft_r2c_noalloc):
         fn.argtypes = [vp, i64, i64, i64, vp, i32, vp]
         fn.restype = ctypes.c_int
+    L.dwcu_server_create.argtypes = [i32, ctypes.c_double, i32, i32, ctypes.POINTER(vp)]
+    L.dwcu_server_create.restype = ctypes.c_int
+    L.dwcu_server_submit.argtypes = [vp, vp, i64, i64, i64, vp, i64, i64, i64, P_opts, vp, ctypes.POINTER(i64)]
+    L.dwcu_server_submit.restype = ctypes.c_int
+    L.dwcu_server_wait.argtypes = [vp, i64, ctypes.c_double, P_opts]
+    L.dwcu_server_wait.restype = ctypes.c_int
+    L.dwcu_server_cancel.argtypes = [vp, i64]
+    L.dwcu_server_cancel.restype = ctypes.c_int
+    L.dwcu_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.dwcu_server_get_stats.restype = ctypes.c_int
+    L.dwcu_server_destroy.argtypes = [vp]
+    L.dwcu_server_destroy.restype = None
     L.dwcu_batch_run.argtypes = [ctypes.POINTER(vp), i32, vp]
     L.dwcu_batch_run.restype = ctypes.c_int
     L.dwcu_psf_prepare.argtypes = [vp, i64, i64, i64, i64, i64, i64, i32, ctypes.c_float, vp,
@@ -337,6 +360,67 @@ def batch_run(jobs: list["Job"], stream: int = 0) -> None:
     """Run set-up jobs to completion together (dwcu_batch_run)."""
     arr = (ctypes.c_void_p * len(jobs))(*[j.h.value for j in jobs])
     _check(lib().dwcu_batch_run(arr, len(jobs), ctypes.c_void_p(stream or None)))
+
+
+class Server:
+    """dwcu_server: continuous batching of deconvolution requests on one GPU.
+
+    ``submit`` queues a dw_function call (host arrays) and returns its id;
+    ``wait`` returns its :class:`Result`.  The arrays are kept referenced
+    until the request is waited for."""
+
+    def __init__(self, device: int = 0, hbm_budget: float = 0.0, max_active: int = 8, iters_per_turn: int = 5):
+        h = ctypes.c_void_p()
+        _check(lib().dwcu_server_create(device, hbm_budget, max_active, iters_per_turn, ctypes.byref(h)))
+        self.h = h
+        self.device = device
+        self._req = {}
+
+    def submit(self, im: np.ndarray, psf: np.ndarray, **kw) -> int:
+        im = np.ascontiguousarray(im, dtype=np.float32)
+        psf = np.ascontiguousarray(psf, dtype=np.float32)
+        kw.setdefault("device", self.device)
+        o = make_opts(**kw)
+        cap = max(o.n_iter, o.maxiter, 1)
+        trace = np.zeros(cap, dtype=np.float32)
+        o.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        o.trace_capacity = cap
+        out = np.empty_like(im)
+        P, N, M = im.shape
+        pP, pN, pM = psf.shape
+        rid = ctypes.c_int64()
+        _check(lib().dwcu_server_submit(self.h, im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP,
+                                        ctypes.byref(o), out.ctypes.data, ctypes.byref(rid)))
+        self._req[rid.value] = (im, psf, out, trace, o)
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0) -> Result:
+        im, psf, out, trace, o = self._req[rid]
+        so = Opts()
+        so.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        so.trace_capacity = len(trace)
+        _check(lib().dwcu_server_wait(self.h, rid, timeout, ctypes.byref(so)))
+        del self._req[rid]
+        return Result(out, trace[: so.iterations_done].copy(), so)
+
+    def cancel(self, rid: int) -> None:
+        _check(lib().dwcu_server_cancel(self.h, rid))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().dwcu_server_get_stats(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self.h:
+            lib().dwcu_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def dw_run(image: np.ndarray, psf: np.ndarray, *, tilesize: int = 0, tilepad: int = 20,

@@ -123,6 +123,142 @@ def synth_image(shape, psf: np.ndarray, K: int, B: int, bg: float, seed: int, wo
     return np.clip(img, 0, 65535).astype(np.uint16).astype(np.float32)
 
 
+def synth_image_blocked(shape, psf: np.ndarray, K: int, B: int, bg: float, seed: int, block: int = 512,
+                        workers: int | None = None) -> np.ndarray:
+    """synth_image for large volumes: the same object model (K points, B
+    blobs, from ``seed``), convolved block by block in x/y (each output block
+    from the object block grown by the PSF half-widths, so the result equals
+    the whole-volume 'same' convolution up to FFT rounding), then Poisson
+    noise per block (a per-block stream derived from ``seed``)."""
+    import scipy.fft as sfft
+    rng = np.random.default_rng(seed)
+    P, N, M = shape
+    obj = np.zeros(shape, dtype=np.float32)
+    idx = (rng.integers(0, P, K), rng.integers(0, N, K), rng.integers(0, M, K))
+    np.add.at(obj, idx, rng.lognormal(7.0, 0.5, K).astype(np.float32))
+    _add_blobs(obj, rng, B)
+    pP, pN, pM = psf.shape
+    hz, hy, hx = (pP - 1) // 2, (pN - 1) // 2, (pM - 1) // 2
+    workers = workers or os.cpu_count() or 1
+    out = np.empty(shape, dtype=np.float32)
+    # object zero-padded by the PSF half widths on every side
+    objp = np.zeros((P + 2 * hz, N + 2 * hy, M + 2 * hx), dtype=np.float32)
+    objp[hz:hz + P, hy:hy + N, hx:hx + M] = obj
+    del obj
+    Fp = {}
+    for y0 in range(0, N, block):
+        for x0 in range(0, M, block):
+            by, bx = min(block, N - y0), min(block, M - x0)
+            sub = objp[:, y0:y0 + by + 2 * hy, x0:x0 + bx + 2 * hx]
+            full = [sfft.next_fast_len(s, real=True) for s in sub.shape]
+            key = tuple(full)
+            if key not in Fp:
+                Fp[key] = sfft.rfftn(psf, s=full, workers=workers)
+            conv = sfft.irfftn(sfft.rfftn(sub, s=full, workers=workers) * Fp[key], s=full, workers=workers)
+            blur = conv[2 * hz:2 * hz + P, 2 * hy:2 * hy + by, 2 * hx:2 * hx + bx]
+            lam = np.clip(bg + blur.astype(np.float64), 0, None)
+            brng = np.random.default_rng([seed, y0, x0])
+            out[:, y0:y0 + by, x0:x0 + bx] = np.clip(brng.poisson(lam), 0, 65535).astype(np.uint16)
+    return out
+
+
+def cached(name: str, cache_dir: str | None, make):
+    """(image, psf) from ``make()``, cached as .npy under cache_dir."""
+    if cache_dir:
+        os.makedirs(cache_dir, exist_ok=True)
+        fi = os.path.join(cache_dir, f"{name}_image.npy")
+        fp = os.path.join(cache_dir, f"{name}_psf.npy")
+        if os.path.exists(fi) and os.path.exists(fp):
+            return np.load(fi), np.load(fp)
+    im, psf = make()
+    if cache_dir:
+        np.save(fi, im)
+        np.save(fp, psf)
+    return im, psf
+
+
+def tiled_inputs(cache_dir: str | None = None):
+    """The 4096 x 4096 x 60 tiled workload: the generator of the 2048 x 2048
+    x 60 workload scaled by area (K = 160000, B = 2400), seed 3, PSF
+    Born-Wolf 670 nm 181 x 181 x 119."""
+    def make():
+        psf = bw_psf((119, 181, 181), lam=670.0)
+        return synth_image_blocked((60, 4096, 4096), psf, 160000, 2400, 100.0, 3), psf
+    return cached("tiles-4096x4096x60", cache_dir, make)
+
+
+CHANNEL_LAMBDAS = (405.0, 466.0, 525.0, 595.0, 670.0, 750.0)
+CHANNEL_ITERS = (20, 40, 60, 80, 100, 150)
+
+
+def channel_spec(c: int):
+    """Channel c of the multi-channel field of view: xy side from 512 to 2048,
+    z from 30 to 80 slices and background 80-150, drawn with seed 40 + c; PSF
+    Born-Wolf at the channel's wavelength, 181 x 181 x (2P - 1)."""
+    rng = np.random.default_rng(40 + c)
+    side = int(rng.choice([512, 768, 1024, 1536, 2048]))
+    P = int(rng.integers(30, 81))
+    bg = float(rng.integers(80, 151))
+    area = side * side * P / (2048 * 2048 * 60)
+    return dict(shape=(P, side, side), psf_shape=(2 * P - 1, 181, 181), lam=CHANNEL_LAMBDAS[c],
+                iters=CHANNEL_ITERS[c], bg=bg, K=max(1, int(40000 * area)), B=max(1, int(600 * area)), seed=40 + c)
+
+
+def channel_inputs(c: int, cache_dir: str | None = None):
+    sp = channel_spec(c)
+
+    def make():
+        psf = bw_psf(sp["psf_shape"], lam=sp["lam"])
+        return synth_image_blocked(sp["shape"], psf, sp["K"], sp["B"], sp["bg"], sp["seed"]), psf
+    return cached(f"channel{c}", cache_dir, make)
+
+
+SERVE_SIZES = ((20, 256, 256), (40, 512, 512), (60, 1024, 1024), (80, 2048, 2048))
+
+
+def serve_requests(n: int, rate: float = 2.0, seed: int = 5):
+    """The serving stream: Poisson arrivals at ``rate`` per second; size class
+    uniform over SERVE_SIZES, wavelength uniform over CHANNEL_LAMBDAS,
+    iterations uniform in [20, 200], SHB or RL with probability 1/2."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    t -= t[0]
+    out = []
+    for i in range(n):
+        out.append(dict(arrival=float(t[i]), size=int(rng.integers(0, len(SERVE_SIZES))),
+                        lam=float(rng.choice(CHANNEL_LAMBDAS)), iters=int(rng.integers(20, 201)),
+                        method="shb" if rng.random() < 0.5 else "rl"))
+    return out
+
+
+def serve_image(size: int, variant: int, cache_dir: str | None = None):
+    """Image ``variant`` (0 or 1) of size class ``size`` (seed 5000 + 10*size
+    + variant), blurred with the 525 nm PSF of that size."""
+    shape = SERVE_SIZES[size]
+    P, N, M = shape
+    area = N * M * P / (2048 * 2048 * 60)
+
+    def make():
+        psf = bw_psf((2 * P - 1, 181, 181), lam=525.0)
+        im = synth_image_blocked(shape, psf, max(1, int(40000 * area)), max(1, int(600 * area)), 100.0,
+                                 5000 + 10 * size + variant)
+        return im, psf
+    return cached(f"serve{size}_{variant}", cache_dir, make)
+
+
+def serve_psf(size: int, lam: float, cache_dir: str | None = None) -> np.ndarray:
+    P = SERVE_SIZES[size][0]
+    if cache_dir:
+        f = os.path.join(cache_dir, f"servepsf{size}_{int(lam)}.npy")
+        if os.path.exists(f):
+            return np.load(f)
+    psf = bw_psf((2 * P - 1, 181, 181), lam=lam)
+    if cache_dir:
+        os.makedirs(cache_dir, exist_ok=True)
+        np.save(f, psf)
+    return psf
+
+
 def config_inputs(name: str, cache_dir: str | None = None):
     """(image, psf) of a named configuration, generated from its seed; cached
     as .npy under cache_dir when given."""

@@ -197,6 +197,43 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P,
                           int64_t tile_size, int64_t overlap, float offset, float xycropfactor,
                           double hbm_budget, dwcu_opts *s, float *out);
 
+/* ---------------------------------------------------------------- serving */
+
+/* A request server on one GPU (no counterpart in the reference, which runs
+ * one image per process): requests are dw_function calls (host image, host
+ * PSF, options, host result buffer) queued from any thread.  A worker thread
+ * admits them in arrival order while their device memory (dwcu_plan_size)
+ * fits hbm_budget bytes (<= 0: 85 % of the free memory) and at most
+ * max_active run, keeps each job's state resident on the device, and
+ * interleaves the jobs' iterations on one stream per job, iters_per_turn
+ * iterations at a time.  A request's result equals dwcu_deconvolve's on the
+ * same inputs.  The caller keeps im, psf and out alive until the request has
+ * finished (dwcu_server_wait). */
+typedef struct dwcu_server dwcu_server;
+typedef struct dwcu_server_stats {
+    int64_t submitted, completed, failed, cancelled, active, queued;
+    double device_bytes_in_use;
+    double latency_p50_s, latency_p99_s, latency_mean_s;  /* submit -> result in the host buffer */
+    double voxel_iterations;  /* sum over completed requests of image voxels x iterations */
+    double wall_s;            /* first submit -> last completion */
+} dwcu_server_stats;
+int dwcu_server_create(int32_t device, double hbm_budget, int32_t max_active, int32_t iters_per_turn,
+                       dwcu_server **server);
+/* Queue one request; *id identifies it.  s->device must be the server's. */
+int dwcu_server_submit(dwcu_server *server, const float *im, int64_t M, int64_t N, int64_t P,
+                       const float *psf, int64_t pM, int64_t pN, int64_t pP, const dwcu_opts *s,
+                       float *out, int64_t *id);
+/* Wait up to timeout_s seconds (< 0: no limit) for a request.  Returns
+ * DWCU_SUCCESS (result in out, outputs in *s_out), DWCU_ERROR_NOT_READY on
+ * timeout, DWCU_ERROR_CANCELLED, or the request's failure status. */
+int dwcu_server_wait(dwcu_server *server, int64_t id, double timeout_s, dwcu_opts *s_out);
+/* Cancel a request: a queued one never starts, a running one stops after
+ * its chunk in flight and releases its memory. */
+int dwcu_server_cancel(dwcu_server *server, int64_t id);
+int dwcu_server_get_stats(dwcu_server *server, dwcu_server_stats *stats);
+/* Cancel queued requests, finish running ones, stop the worker. */
+void dwcu_server_destroy(dwcu_server *server);
+
 /* ---------------------------------------------------------------- FFT */
 
 /* 3-D real-to-complex transform of d_in (M x N x P floats, device) into

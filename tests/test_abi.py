@@ -84,3 +84,15 @@ def test_no_gpu_no_fallback():
         dw.run_method(im, psf, n_iter=3)
     assert e.value.code == 4
     assert "no CUDA device" in str(e.value)
+
+
+@pytest.mark.skipif(dw.lib().dwcu_device_count() > 0, reason="a GPU is present")
+def test_no_gpu_server_and_tiles_fail():
+    with pytest.raises(dw.DwcuError) as e:
+        dw.Server()
+    assert e.value.code == 4
+    im = np.ones((4, 40, 40), np.float32) * 100
+    psf = np.ones((3, 3, 3), np.float32) / 27
+    with pytest.raises(dw.DwcuError) as e:
+        dw.deconvolve_tiled(im, psf, 20, 4, n_iter=2)
+    assert e.value.code == 4
