@@ -28,7 +28,9 @@ __all__ = [
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdwcu.so")
+# the engine library (DWCU_LIBRARY names another build of it, e.g. one
+# compiled for a subset of transform lengths)
+LIB_PATH = os.environ.get("DWCU_LIBRARY") or os.path.join(HERE, "libdwcu.so")
 
 METHOD_RL, METHOD_SHB = 0, 2
 ITER_ABS, ITER_REL, ITER_FIXED = 0, 1, 2
@@ -123,7 +125,7 @@ EXPORTS = [
     "dwcu_profile_enable", "dwcu_profile_collect", "dwcu_batch_run", "dwcu_psf_prepare",
     "dwcu_tiling_create", "dwcu_deconvolve_tiled", "dwcu_fft_r2c_noalloc", "dwcu_server_create",
     "dwcu_server_submit", "dwcu_server_wait", "dwcu_server_cancel", "dwcu_server_get_stats",
-    "dwcu_server_destroy",
+    "dwcu_server_destroy", "dwcu_tile_blend",
 ]
 
 _lib = None
@@ -188,6 +190,8 @@ def lib() -> ctypes.CDLL:
     L.dwcu_server_get_stats.restype = ctypes.c_int
     L.dwcu_server_destroy.argtypes = [vp]
     L.dwcu_server_destroy.restype = None
+    L.dwcu_tile_blend.argtypes = [vp, i64, i64, i64, ctypes.POINTER(Tile), i32, i32, vp, ctypes.c_float, i32, vp]
+    L.dwcu_tile_blend.restype = ctypes.c_int
     L.dwcu_batch_run.argtypes = [ctypes.POINTER(vp), i32, vp]
     L.dwcu_batch_run.restype = ctypes.c_int
     L.dwcu_psf_prepare.argtypes = [vp, i64, i64, i64, i64, i64, i64, i32, ctypes.c_float, vp,
@@ -354,6 +358,25 @@ def deconvolve_tiled(im: np.ndarray, psf: np.ndarray, tile_size: int, overlap: i
                                        overlap, offset, xycropfactor, hbm_budget, ctypes.byref(o),
                                        out.ctypes.data))
     return Result(out, np.zeros(0, np.float32), o)
+
+
+def tiles_array(tiles: list[dict]):
+    """The ctypes array of dwcu_tile for tiles as tiling_create returns them."""
+    arr = (Tile * len(tiles))()
+    for a, t in zip(arr, tiles):
+        for k in ("size", "pos", "xpos", "xsize"):
+            getattr(a, k)[:] = list(t[k])
+    return arr
+
+
+def tile_blend_device(d_out: int, shape, tiles, tid: int, d_tile: int, offset: float = 5.0, device: int = 0,
+                      stream: int = 0) -> None:
+    """dwcu_tile_blend on device buffers; ``tiles`` from :func:`tiling_create`
+    (or a :func:`tiles_array`)."""
+    P, N, M = shape
+    arr = tiles if not isinstance(tiles, list) else tiles_array(tiles)
+    _check(lib().dwcu_tile_blend(ctypes.c_void_p(d_out), M, N, P, arr, len(arr), tid, ctypes.c_void_p(d_tile),
+                                 offset, device, ctypes.c_void_p(stream or None)))
 
 
 def batch_run(jobs: list["Job"], stream: int = 0) -> None:

@@ -411,4 +411,41 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, cons
     return rc;
 }
 
+int dwcu_tile_blend(float *d_out, int64_t M, int64_t N, int64_t P, const dwcu_tile *tiles, int32_t ntiles,
+                    int32_t tid, const float *d_tile, float offset, int32_t device, void *stream)
+{
+    if (!d_out || !tiles || !d_tile) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    if (ntiles < 1 || tid < 0 || tid >= ntiles) return fail(DWCU_ERROR_INVALID_VALUE, "bad tile index");
+    for (int i = 0; i < ntiles; ++i) {
+        const dwcu_tile &t = tiles[i];
+        if (t.xpos[0] < 0 || t.xpos[1] >= M || t.xpos[2] < 0 || t.xpos[3] >= N || t.xpos[4] < 0 || t.xpos[5] >= P ||
+            t.xsize[0] != t.xpos[1] - t.xpos[0] + 1 || t.xsize[1] != t.xpos[3] - t.xpos[2] + 1 ||
+            t.xsize[2] != t.xpos[5] - t.xpos[4] + 1)
+            return fail(DWCU_ERROR_INVALID_VALUE, "tile %d does not lie in the image", i);
+    }
+    HCU(cudaSetDevice(device));
+    cudaStream_t st = (cudaStream_t) stream;
+    std::vector<DevTile> ht((size_t) ntiles);
+    for (int i = 0; i < ntiles; ++i) {
+        memcpy(ht[(size_t) i].pos, tiles[i].pos, sizeof ht[0].pos);
+        memcpy(ht[(size_t) i].xpos, tiles[i].xpos, sizeof ht[0].xpos);
+        memcpy(ht[(size_t) i].xsize, tiles[i].xsize, sizeof ht[0].xsize);
+    }
+    DevTile *d_tiles = nullptr;
+    HCU(cudaMalloc(&d_tiles, sizeof(DevTile) * (size_t) ntiles));
+    cudaError_t e = cudaMemcpyAsync(d_tiles, ht.data(), sizeof(DevTile) * (size_t) ntiles, cudaMemcpyHostToDevice, st);
+    const dwcu_tile &t = tiles[tid];
+    const size_t tv = (size_t) (t.xsize[0] * t.xsize[1] * t.xsize[2]);
+    if (e == cudaSuccess) {
+        const int blocks = (int) std::min<size_t>(4096, (tv + 255) / 256);
+        k_tile_blend<<<blocks, 256, 0, st>>>(d_tile, M, N, d_tiles, ntiles, tid, offset, d_out);
+        dwcu::record_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_tiles);
+    if (e != cudaSuccess) return fail(DWCU_ERROR_CUDA, "tile blend failed: %s", cudaGetErrorString(e));
+    return DWCU_SUCCESS;
+}
+
 }  // extern "C"

@@ -197,6 +197,15 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P,
                           int64_t tile_size, int64_t overlap, float offset, float xycropfactor,
                           double hbm_budget, dwcu_opts *s, float *out);
 
+/* Blend one deconvolved tile (device buffer d_tile, tiles[tid].xsize) into the
+ * device volume d_out (M x N x P): minus offset and clipped at 0 when
+ * offset > 0 (dw.c:2141-2145), then out += w / sum_w * tile with the weights
+ * of tiling_put_tile (src/tiling.c:412-439).  Tiles blended in tile order give
+ * deconvolve_tiles' result; tiles spread over several GPUs can be blended
+ * per GPU and the volumes summed.  Synchronises the stream. */
+int dwcu_tile_blend(float *d_out, int64_t M, int64_t N, int64_t P, const dwcu_tile *tiles, int32_t ntiles,
+                    int32_t tid, const float *d_tile, float offset, int32_t device, void *stream);
+
 /* ---------------------------------------------------------------- serving */
 
 /* A request server on one GPU (no counterpart in the reference, which runs

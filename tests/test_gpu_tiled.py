@@ -99,3 +99,20 @@ def test_batch_run_equals_one_at_a_time():
         assert r.iterations == ref.iterations
         np.testing.assert_array_equal(r.out, ref.out)
         np.testing.assert_array_equal(r.trace, ref.trace)
+
+
+def test_multi_layer_single_rank_equals_batched():
+    """The multi-GPU layer run in one process (tiles one by one through
+    dwcu_deconvolve, blended on the device by dwcu_tile_blend) gives the
+    batched tiled result exactly."""
+    from deconwolf_b200 import multi
+    im, psf = _inputs(seed=15)
+    pp = dw.psf_prepare(psf, im.shape)
+    a = dw.deconvolve_tiled(im, pp, 30, 6, n_iter=7).out
+    b = multi.deconvolve_tiled(im, pp, 30, 6, n_iter=7)
+    np.testing.assert_array_equal(a, b)
+    jobs = [dict(image=im[:, :40, :40].copy(), psf=psf, kw=dict(n_iter=4)),
+            dict(image=im[:, 20:, 10:].copy(), psf=psf, kw=dict(n_iter=3, method="rl"))]
+    res = multi.run_jobs(jobs)
+    for j, r in zip(jobs, res):
+        np.testing.assert_array_equal(r, dw.run_method(j["image"], j["psf"], **j["kw"]).out)
