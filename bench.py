@@ -375,7 +375,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD,
-                    choices=[WORKLOAD, SMALL, PROFILE_CASE, "tiles-4096x4096x60", "channels-6", "serve-stream"])
+                    choices=[WORKLOAD, SMALL, PROFILE_CASE, "shb-2048x256x20", "shb-256x2048x20", "shb-256x256x60",
+                             "tiles-4096x4096x60", "channels-6", "serve-stream"])
     ap.add_argument("--tilesize", type=int, default=1024)
     ap.add_argument("--requests", type=int, default=60, help="serve-stream: number of requests (full stream: 500)")
     ap.add_argument("--hbm-budget", type=float, default=160e9, help="serve-stream: device bytes for admitted jobs")

@@ -52,7 +52,8 @@ void launch_lines_t(const LinesArgs &a, int nblocks, cudaStream_t st)
     using C = LinesCfg<RD, T>;
     ensure_smem(ko, k_lines<RD, T>, C::SMEM_BYTES);
     constexpr int tpl = C::THREADS / T;
-    k_lines<RD, T><<<nblocks, dim3(T, tpl), C::SMEM_BYTES, st>>>(a);
+    const size_t smem = a.mode >= LINES_CONV ? C::SMEM_BYTES : C::SMEM_FFT;
+    k_lines<RD, T><<<nblocks, dim3(T, tpl), smem, st>>>(a);
 }
 
 template <class RD, int DIR>

@@ -178,8 +178,10 @@ struct LinesArgs {
 template <class RD, int T>
 struct LinesCfg {
     static constexpr int THREADS = T * cmax(RD::TPL, RevRad<RD>::TPL);
-    static constexpr size_t SMEM_BYTES =
-        sizeof(float2) * (size_t) cmax(RD::PADN, RevRad<RD>::PADN) * T;
+    // exchange tile, then (convolve modes) the OTF tile, prefetched at entry
+    static constexpr int XCH_F2 = cmax(RD::PADN, RevRad<RD>::PADN) * T;
+    static constexpr size_t SMEM_FFT = sizeof(float2) * (size_t) XCH_F2;
+    static constexpr size_t SMEM_BYTES = SMEM_FFT + sizeof(float2) * (size_t) RD::N * T;
     // aim for three resident CTAs when threads and shared memory allow
     static constexpr int MIN_BLOCKS =
         (THREADS * 3 <= 2048 && SMEM_BYTES * 3 <= 225 * 1024) ? 3 : (THREADS * 2 <= 2048 ? 2 : 1);
@@ -203,6 +205,21 @@ k_lines(LinesArgs a)
     const long long ls = a.line_stride;
     const int mode = a.mode;
     auto smem = [&](int, int i) { return sm + (size_t) i * T + line; };
+    using Cfg = LinesCfg<RD, T>;
+    float2 *sotf = sm + Cfg::XCH_F2;  // OTF tile [n][col] (convolve modes)
+    const int col0 = tile * T;
+    if (mode >= LINES_CONV && (T % 2) == 0) {
+        // the tile's OTF columns arrive while the forward transform runs:
+        // 16-byte pieces (two columns) of each of the N rows
+        const int tid = t * T + line;
+        const float2 *h0 = a.otf + outer * a.outer_stride + col0;
+        constexpr int PPR = T / 2;  // pieces per row
+        for (int e = tid; e < N * PPR; e += Cfg::THREADS) {
+            const int n = e / PPR, p = e - n * PPR;
+            if (col0 + 2 * p < a.ncols) cp_async16(sotf + n * T + 2 * p, h0 + (long long) n * ls + 2 * p);
+        }
+        cp_async_commit();
+    }
 
     float2 v[1][RD::RA];
     if (t < N / RD::RA) {
@@ -227,7 +244,17 @@ k_lines(LinesArgs a)
         return;
     }
     // multiply by the OTF (conjugated for the back-projection)
-    if (t < SL && valid) {
+    if constexpr ((T % 2) == 0) {
+        cp_async_wait_all();
+        __syncthreads();  // every thread's pieces of the OTF tile have landed
+        if (t < SL && valid) {
+#pragma unroll
+            for (int r = 0; r < RD::RL; ++r) {
+                const float2 q = sotf[(t + r * SL) * T + line];
+                o[0][r] = (mode == LINES_CONV) ? cmul(o[0][r], q) : cmulc(o[0][r], q);
+            }
+        }
+    } else if (t < SL && valid) {
         const float2 *h = a.otf + off;
 #pragma unroll
         for (int r = 0; r < RD::RL; ++r) {

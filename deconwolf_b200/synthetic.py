@@ -78,6 +78,15 @@ CONFIGS = {
     # buffers > L2, a few GB on the device): used for hardware-counter captures
     "shb-1024x1024x20": dict(shape=(20, 1024, 1024), psf_shape=(39, 181, 181), lam=670.0, K=3300, B=50, bg=100.0,
                              seed=3),
+    # small cases whose x, y or z transform length is that of the 2048^2 x 60
+    # workload (2240, 2240, 180), so one axis's kernel is exactly the one it
+    # runs, on ~1 GB of device memory: hardware-counter captures
+    "shb-2048x256x20": dict(shape=(20, 256, 2048), psf_shape=(39, 181, 181), lam=670.0, K=800, B=12, bg=100.0,
+                            seed=4),
+    "shb-256x2048x20": dict(shape=(20, 2048, 256), psf_shape=(39, 181, 181), lam=670.0, K=800, B=12, bg=100.0,
+                            seed=5),
+    "shb-256x256x60": dict(shape=(60, 256, 256), psf_shape=(119, 181, 181), lam=670.0, K=600, B=9, bg=100.0,
+                           seed=6),
 }
 
 
