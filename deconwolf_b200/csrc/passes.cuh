@@ -777,11 +777,15 @@ k_xpass(XArgs a)
         // Im X[0] and Im X[L] are ignored, as by any real inverse transform
         float2 v[Q][RD::RA];
         if (t < L / RD::RA) {
-#pragma unroll
-            for (int r = 0; r < RD::RA; ++r) {
+            // W_X^k for k = t + r*L/RA: one table value, times compile-time
+            // factors W_X^{r*L/RA} (the table stays out of the L1 cache,
+            // which the staging buffers leave small)
+            const float2 tb = __ldg(&a.tw[t]);
+            static_for<RD::RA>([&](auto rc) {
+                constexpr int r = decltype(rc)::value;
                 const int k = t + r * (L / RD::RA);
                 const int km = L - k;
-                const float2 tk = __ldg(&a.tw[k]);
+                const float2 tk = twiddle<C::X, r * (L / RD::RA), -1>(tb);
                 const int ik = (k / KB) * (R * KB) + (k % KB);
                 const int im = (km / KB) * (R * KB) + (km % KB);
 #pragma unroll
@@ -795,7 +799,7 @@ k_xpass(XArgs a)
                     float2 e = cmulc(d, tk);
                     v[q][r] = make_float2(s.x - e.y, s.y + e.x);
                 }
-            }
+            });
         }
         __syncthreads();  // the staged rows become the exchange tiles
         line_fft<RD, +1, Q, true>(v, w, t, a.twL, smem);
@@ -850,20 +854,48 @@ k_xpass(XArgs a)
     // ---- Hermitian post-processing X[k] = E[k] + W_X^k O[k], k = 0..L,
     // written to the blocked layout: thread e -> (kb, row, ki)
     float2 *Sz = a.S + (long long) z * plane + (long long) y0 * KB;
-    for (int e = tid; e < C::NKB * R * KB; e += C::THREADS) {
-        const int ki = e % KB;
-        const int r2 = (e / KB) % R;
-        const int kb = e / (KB * R);
-        const int k = kb * KB + ki;
-        if (k > L || y0 + r2 >= a.Y) continue;
+    constexpr int TOT = C::NKB * R * KB;
+    if constexpr (C::THREADS % (KB * R) == 0) {
+        // thread tid handles e = tid + m*THREADS: one row, k = k0 + m*THREADS/R,
+        // so W_X^k = W_X^{k0} times compile-time factors
+        constexpr int DK = C::THREADS / R;
+        constexpr int MAXM = (TOT + C::THREADS - 1) / C::THREADS;
+        const int ki0 = tid % KB;
+        const int r2 = (tid / KB) % R;
+        const int k0 = (tid / (KB * R)) * KB + ki0;
+        const float2 tb = __ldg(&a.tw[k0 <= L ? k0 : 0]);
         const float2 *Br = CB + (size_t) r2 * C::ROW_F2;
-        float2 zk = Br[k == L ? 0 : k];
-        float2 zm = Br[k == 0 ? 0 : L - k];
-        zm.y = -zm.y;
-        float2 ev = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
-        float2 d = csub(zk, zm);
-        float2 o = make_float2(0.5f * d.y, -0.5f * d.x);  // -(i/2) d
-        Sz[(long long) kb * a.Y * KB + r2 * KB + ki] = cadd(ev, cmul(o, __ldg(&a.tw[k])));
+        const bool row_ok = y0 + r2 < a.Y;
+        static_for<MAXM>([&](auto mc) {
+            constexpr int m = decltype(mc)::value;
+            const int k = k0 + m * DK;
+            if (tid + m * C::THREADS < TOT && k <= L && row_ok) {
+                float2 zk = Br[k == L ? 0 : k];
+                float2 zm = Br[k == 0 ? 0 : L - k];
+                zm.y = -zm.y;
+                float2 ev = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+                float2 d = csub(zk, zm);
+                float2 o = make_float2(0.5f * d.y, -0.5f * d.x);  // -(i/2) d
+                const int kb = k / KB;
+                Sz[(long long) kb * a.Y * KB + r2 * KB + ki0] = cadd(ev, cmul(o, twiddle<C::X, m * DK, -1>(tb)));
+            }
+        });
+    } else {
+        for (int e = tid; e < TOT; e += C::THREADS) {
+            const int ki = e % KB;
+            const int r2 = (e / KB) % R;
+            const int kb = e / (KB * R);
+            const int k = kb * KB + ki;
+            if (k > L || y0 + r2 >= a.Y) continue;
+            const float2 *Br = CB + (size_t) r2 * C::ROW_F2;
+            float2 zk = Br[k == L ? 0 : k];
+            float2 zm = Br[k == 0 ? 0 : L - k];
+            zm.y = -zm.y;
+            float2 ev = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+            float2 d = csub(zk, zm);
+            float2 o = make_float2(0.5f * d.y, -0.5f * d.x);  // -(i/2) d
+            Sz[(long long) kb * a.Y * KB + r2 * KB + ki] = cadd(ev, cmul(o, __ldg(&a.tw[k])));
+        }
     }
 }
 
