@@ -205,6 +205,15 @@ __host__ __device__ constexpr int dft_first_factor(int n)
     return (n % 4 == 0 && n != 8) ? 4 : (n % 2 == 0 ? 2 : (n % 3 == 0 ? 3 : (n % 5 == 0 ? 5 : 7)));
 }
 
+__host__ __device__ constexpr int cgcd(int a, int b) { return b == 0 ? a : cgcd(b, a % b); }
+// inverse of a modulo m (gcd(a, m) == 1)
+__host__ __device__ constexpr int cinv(int a, int m)
+{
+    int r = 1;
+    while ((a * r) % m != 1 % m) ++r;
+    return r % m;
+}
+
 template <int N, int DIR>
 struct Dft {
     static constexpr int A = dft_first_factor(N);
@@ -212,6 +221,41 @@ struct Dft {
     static_assert(A * B == N, "length must be 7-smooth");
     static DW_HD void run(float2 *v)
     {
+        if constexpr (cgcd(A, B) == 1) {
+            // prime-factor (Good-Thomas) algorithm: input n = (a*B + b*A) mod N,
+            // output k = (ka*B*(B^-1 mod A) + kb*A*(A^-1 mod B)) mod N; the
+            // sub-transforms need no twiddle factors
+            constexpr int CA = B * cinv(B % A, A);  // = 1 mod A, 0 mod B
+            constexpr int CB = A * cinv(A % B, B);  // = 0 mod A, 1 mod B
+            float2 t[N];
+            static_for<B>([&](auto bb) {
+                constexpr int b = decltype(bb)::value;
+                float2 u[A];
+                static_for<A>([&](auto aa) {
+                    constexpr int a = decltype(aa)::value;
+                    u[a] = v[(a * B + b * A) % N];
+                });
+                Dft<A, DIR>::run(u);
+                static_for<A>([&](auto kk) {
+                    constexpr int ka = decltype(kk)::value;
+                    t[ka * B + b] = u[ka];
+                });
+            });
+            static_for<A>([&](auto kk) {
+                constexpr int ka = decltype(kk)::value;
+                float2 w[B];
+                static_for<B>([&](auto bb) {
+                    constexpr int b = decltype(bb)::value;
+                    w[b] = t[ka * B + b];
+                });
+                Dft<B, DIR>::run(w);
+                static_for<B>([&](auto bb) {
+                    constexpr int kb = decltype(bb)::value;
+                    v[(ka * CA + kb * CB) % N] = w[kb];
+                });
+            });
+            return;
+        }
         float2 t[N];
         // A-point DFTs over the subsequences v[b + B*a]
         static_for<B>([&](auto bb) {
