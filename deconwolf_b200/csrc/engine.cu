@@ -520,7 +520,9 @@ static int pass_y(dwcu_job *j, int mode, float2 *data, long long planes = -1)
         a.err = &j->sc->flags;
         a.ntiles = (int) (planes * g.NKB);
         a.dir = (mode == LINES_INV) ? +1 : -1;
-        ProfScope ps(mode == LINES_INV ? "y_inv" : "y_fwd", 16.0 * (double) g.NKB * KB * g.Y * planes, j->stream);
+        // the passes over the image planes only are timed as their own class
+        const char *nm = mode == LINES_INV ? (planes < g.Z ? "y_inv_img" : "y_inv") : (planes < g.Z ? "y_fwd_img" : "y_fwd");
+        ProfScope ps(nm, 16.0 * (double) g.NKB * KB * g.Y * planes, j->stream);
         g.ytp->launch(a, j->stream);
         CHECK_LAUNCH();
         return DWCU_SUCCESS;
