@@ -84,13 +84,31 @@ void launch_x_fam(const XArgs &a, cudaStream_t st)
     k_xpass<RD, R, FAM><<<a.ntiles, dim3(C::TPL, C::RY), C::SMEM_BYTES, st>>>(a);
 }
 
+// The forward and update families always run over every row; where the
+// plan's tiles hold two rows and one row still fills two warps, they run one
+// row per CTA (half the shared memory and threads per CTA, twice the CTAs per
+// SM to hide each other's barriers).  The ratio and store families keep the
+// plan's tiles (the ratio's error partials are counted per plan tile).
+template <class RD, int R, int FAM>
+void launch_x_rows(const XArgs &a, cudaStream_t st)
+{
+    constexpr int row_threads = cmax(RD::TPL, RevRad<RD>::TPL);
+    if constexpr (R == 2 && row_threads >= 64) {
+        XArgs b = a;
+        b.ntiles = a.Z * a.Y;
+        launch_x_fam<RD, 1, FAM>(b, st);
+    } else {
+        launch_x_fam<RD, R, FAM>(a, st);
+    }
+}
+
 template <class RD, int R>
 void launch_x_t(const XArgs &a, cudaStream_t st)
 {
     switch (x_family(a.op)) {
-    case XFAM_FWD: launch_x_fam<RD, R, XFAM_FWD>(a, st); break;
+    case XFAM_FWD: launch_x_rows<RD, R, XFAM_FWD>(a, st); break;
     case XFAM_RATIO: launch_x_fam<RD, R, XFAM_RATIO>(a, st); break;
-    case XFAM_UPDATE: launch_x_fam<RD, R, XFAM_UPDATE>(a, st); break;
+    case XFAM_UPDATE: launch_x_rows<RD, R, XFAM_UPDATE>(a, st); break;
     default: launch_x_fam<RD, R, XFAM_STORE>(a, st); break;
     }
 }
