@@ -452,7 +452,9 @@ struct XCfg {
     static constexpr size_t RED_OFF = REAL_OFF + x_slots(FAM) * sizeof(float) * (size_t) REAL_F;
     static constexpr size_t SMEM_BYTES = RED_OFF + sizeof(double) * THREADS;
     // resident CTAs per SM to aim for (registers are capped to fit them)
-    static constexpr int MIN_BLOCKS = (SMEM_BYTES * 4 <= 224 * 1024 && THREADS * 4 <= 2048) ? 4
+    // (one-row update tiles, family 2: five CTAs, which caps registers at 72)
+    static constexpr int MIN_BLOCKS = (R == 1 && FAM == 2 && SMEM_BYTES * 5 <= 224 * 1024 && THREADS * 5 <= 2048) ? 5
+                                    : (SMEM_BYTES * 4 <= 224 * 1024 && THREADS * 4 <= 2048) ? 4
                                     : (SMEM_BYTES * 3 <= 225 * 1024 && THREADS * 3 <= 2048) ? 3 : 1;
     static_assert(R % Q == 0, "rows per tile");
     static_assert(THREADS >= 32, "the error reduction needs one full warp");
@@ -678,6 +680,9 @@ k_xpass(XArgs a)
 {
     using C = XCfg<RD, R, FAM>;
     using RV = typename C::RV;
+    // twiddles loaded ahead of the barriers cost registers across them; the
+    // ratio family (four CTAs per SM, few registers) loads them in place
+    constexpr bool PREF_TW = (FAM != XFAM_RATIO);
     constexpr int L = C::L;
     constexpr int Q = C::Q;
     constexpr int XP = C::XP;       // real row pitch (a.X == XP)
@@ -803,7 +808,7 @@ k_xpass(XArgs a)
             });
         }
         __syncthreads();  // the staged rows become the exchange tiles
-        line_fft<RD, +1, Q, true>(v, w, t, a.twL, smem);
+        line_fft<RD, +1, Q, PREF_TW>(v, w, t, a.twL, smem);
     }
     if (!wait_all(&bars[1], 0, a.err, 3 << 8)) return;
 
@@ -842,7 +847,7 @@ k_xpass(XArgs a)
     // ---- forward with the reversed radix list; w is its first-stage input
     __syncthreads();  // all reads of the exchange tiles are complete
     float2 qo[Q][RV::RL];
-    line_fft<RV, -1, Q, true>(w, qo, t, a.twL, smem);
+    line_fft<RV, -1, Q, PREF_TW>(w, qo, t, a.twL, smem);
     constexpr int SQ = L / RV::RL;
     __syncthreads();
     if (t < SQ) {
