@@ -1098,6 +1098,9 @@ static int job_result(dwcu_job *j, float *out, bool on_device, dwcu_opts *so)
 // the graph holds independent chains, so small jobs (tiles, channels) share
 // the GPU instead of running one after another.  Jobs with a REL/ABS stopping
 // rule are stepped round-robin, one iteration each, on their own streams.
+// padded job voxels from which one job's passes fill every SM
+constexpr double kBatchLargeJob = 32.0 * 1024 * 1024;
+
 static int batch_run(dwcu_job **jobs, int n, cudaStream_t origin)
 {
     if (n <= 0) return DWCU_SUCCESS;
@@ -1144,8 +1147,20 @@ static int batch_run(dwcu_job **jobs, int n, cudaStream_t origin)
         cudaGraph_t gr = nullptr;
         if (graph) CU(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal));
         cudaEventRecord(fork, origin);
+        // Jobs that fill the GPU on their own run one after another on one
+        // chain: side by side they would only compete for the SMs and evict
+        // each other's data from L2 between passes.  Smaller jobs run as
+        // chains of their own beside them.
+        int big_chain = -1;
         for (int i : fixed_idx) {
             dwcu_job *j = jobs[i];
+            const double vox = (double) j->g.X * (double) j->g.Y * (double) j->g.Z;
+            if (vox >= kBatchLargeJob) {
+                if (big_chain < 0)
+                    big_chain = i;
+                else
+                    j->stream = streams[(size_t) big_chain];
+            }
             cudaStreamWaitEvent(j->stream, fork, 0);
             const int ug = j->s.use_graph;
             j->s.use_graph = 0;  // eager launches: captured into the batch graph

@@ -182,10 +182,11 @@ struct LinesCfg {
     static constexpr int XCH_F2 = cmax(RD::PADN, RevRad<RD>::PADN) * T;
     static constexpr size_t SMEM_FFT = sizeof(float2) * (size_t) XCH_F2;
     static constexpr size_t SMEM_BYTES = SMEM_FFT + sizeof(float2) * (size_t) RD::N * T;
-    // four resident CTAs when that leaves at least 64 registers a thread
+    // as many resident CTAs (up to four) as leave at least 64 registers a thread
     static constexpr int MIN_BLOCKS =
         (THREADS * 4 <= 1024 && SMEM_BYTES * 4 <= 225 * 1024) ? 4
-        : (THREADS * 3 <= 2048 && SMEM_BYTES * 3 <= 225 * 1024) ? 3 : (THREADS * 2 <= 2048 ? 2 : 1);
+        : (THREADS * 3 <= 1024 && SMEM_BYTES * 3 <= 225 * 1024) ? 3
+        : (THREADS * 2 <= 1024 && SMEM_BYTES * 2 <= 225 * 1024) ? 2 : 1;
 };
 
 template <class RD, int T>

@@ -132,9 +132,10 @@ int dwcu_job_setup(dwcu_job *job, const float *im, const float *psf, int32_t on_
  * per iteration).  *remaining receives how many iterations may still run. */
 int dwcu_job_step(dwcu_job *job, int32_t n, int32_t *remaining);
 /* Run set-up jobs to completion together: jobs with a fixed iteration count
- * become independent chains of one CUDA graph (one stream each), so tiles
- * and channels of uneven sizes share the GPU; REL/ABS jobs are stepped
- * round-robin.  Replaces the sequential tile loop of deconvolve_tiles
+ * become chains of one CUDA graph: jobs large enough to fill the GPU
+ * (>= 32 Mi padded voxels) one after another on one chain, smaller ones on
+ * chains of their own beside them, so tiles and channels of uneven sizes
+ * share the GPU; REL/ABS jobs are stepped round-robin.  Replaces the sequential tile loop of deconvolve_tiles
  * (src/dw.c:2093-2153) for the iteration part.  Returns when all are done;
  * results are then read with dwcu_job_result. */
 int dwcu_batch_run(dwcu_job **jobs, int32_t n, void *stream);
