@@ -269,6 +269,28 @@ static int get_ctx(int device, DeviceCtx **out)
     return DWCU_SUCCESS;
 }
 
+// gaussian_kernel (fim.c:2077-2106): 2*ceil(3 sigma)+1 taps with the
+// reference's mixed float/double arithmetic, normalised to sum 1
+static GaussTaps gauss_taps(float sigma)
+{
+    GaussTaps K{};
+    int len = (int) std::ceil(3.0 * sigma);
+    if (len < 1) len = 1;
+    const int n = 2 * len + 1;
+    K.n = n;
+    const float mid = (n - 1) / 2;
+    const float s2 = (float) std::pow((double) sigma, 2.0);
+    const float k0 = (float) (1.0 / sigma / std::sqrt(2.0 * M_PI));
+    double sum = 0;
+    for (int kk = 0; kk < n; ++kk) {
+        const float x = (float) kk - mid;
+        K.k[kk] = (float) ((double) k0 * std::exp(-0.5 * std::pow((double) x, 2.0) / (double) s2));
+        sum += K.k[kk];
+    }
+    for (int kk = 0; kk < n; ++kk) K.k[kk] = (float) ((double) K.k[kk] / sum);
+    return K;
+}
+
 // twiddle table of a length, evaluated in double from the exact angle
 // reduction in dft.cuh and rounded once to float
 static int get_twiddles(DeviceCtx *c, long long n, const float2 **out)
@@ -755,9 +777,8 @@ static int check_opts(const dwcu_opts &s)
         return fail(DWCU_ERROR_INVALID_VALUE, "method must be SHB (2) or RL (0), got %d", s.method);
     if (s.iter_type < 0 || s.iter_type > 2) return fail(DWCU_ERROR_INVALID_VALUE, "bad iter_type %d", s.iter_type);
     if (s.n_iter < 0 || s.maxiter < 0) return fail(DWCU_ERROR_INVALID_VALUE, "negative iteration count");
-    if (s.start_condition == DWCU_START_LP)
-        return fail(DWCU_ERROR_UNSUPPORTED, "start_condition LP (Gaussian low-pass start) is not implemented");
-    if (s.start_condition != DWCU_START_FLAT && s.start_condition != DWCU_START_IDENTITY)
+    if (s.start_condition != DWCU_START_FLAT && s.start_condition != DWCU_START_IDENTITY &&
+        s.start_condition != DWCU_START_LP)
         return fail(DWCU_ERROR_INVALID_VALUE, "bad start_condition %d", s.start_condition);
     if (s.metric != DWCU_METRIC_IDIV && s.metric != DWCU_METRIC_MSE)
         return fail(DWCU_ERROR_INVALID_VALUE, "bad metric %d", s.metric);
@@ -855,6 +876,37 @@ static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_dev
     const int fb = (int) std::min<long long>(148 * 16, (nv + 255) / 256);
     if (j->s.start_condition == DWCU_START_FLAT) {
         k_fill_scalar<<<fb, 256, 0, st>>>(j->xa, nv, j->sc);
+        CHECK_LAUNCH();
+    } else if (j->s.start_condition == DWCU_START_LP) {
+        // method_shb.c:278-285, method_rl.c:290-297: the image smoothed by
+        // fim_gsmooth(sigma 8), inserted at the corner.  x_{k-1} and the
+        // spectrum are free here and hold the intermediate volumes.
+        const long long nimg = g.M * g.N * g.P;
+        const int gb = (int) std::min<long long>(148 * 16, (nimg + 255) / 256);
+        float *t1 = j->xb, *t2 = reinterpret_cast<float *>(j->S);
+        GaussTaps K = gauss_taps(8.0f);
+        CU(cudaMemcpy2DAsync(t2, sizeof(float) * g.M, j->gimg, sizeof(float) * g.GP, sizeof(float) * g.M,
+                             g.N * g.P, cudaMemcpyDeviceToDevice, st));
+        k_gsmooth_axis<<<gb, 256, 0, st>>>(t2, t1, (int) g.M, (int) g.N, (int) g.P, 0, K);
+        CHECK_LAUNCH();
+        k_gsmooth_axis<<<gb, 256, 0, st>>>(t1, t2, (int) g.M, (int) g.N, (int) g.P, 1, K);
+        CHECK_LAUNCH();
+        const float *lp = t2;
+        if (g.P > 1) {
+            // fim_gsmooth_aniso trims the z kernel to at most 2P-1 taps
+            GaussTaps Kz = K;
+            int off = 0;
+            while (Kz.n > 2 * g.P - 1) {
+                ++off;
+                Kz.n -= 2;
+            }
+            for (int i = 0; i < Kz.n; ++i) Kz.k[i] = K.k[i + off];
+            k_gsmooth_axis<<<gb, 256, 0, st>>>(t2, t1, (int) g.M, (int) g.N, (int) g.P, 2, Kz);
+            CHECK_LAUNCH();
+            lp = t1;
+        }
+        CU(cudaMemsetAsync(j->xa, 0, R, st));
+        k_embed_image<<<fb, 256, 0, st>>>(lp, g.M, (int) g.M, (int) g.N, (int) g.P, j->xa, (int) g.XP, (int) g.Y);
         CHECK_LAUNCH();
     } else {
         CU(cudaMemsetAsync(j->xa, 0, R, st));

@@ -199,6 +199,59 @@ __global__ void k_embed_image(const float *__restrict__ g, long long GP, int M, 
     }
 }
 
+// One axis of fim_gsmooth (fim.c:2240-2278): each line convolved with the
+// taps as fim_conv1_vector does it with normalized = 1 (fim.c:1944-2066):
+// float products summed in double in tap order, the kernel renormalised by
+// the sum of the taps that fall inside the line, one rounding to float.
+// in and out are M x N x P, x fastest; axis 0, 1, 2 = x, y, z.
+struct GaussTaps {
+    float k[64];
+    int n;
+};
+__global__ void k_gsmooth_axis(const float *__restrict__ in, float *__restrict__ out, int M, int N, int P, int axis,
+                               GaussTaps K)
+{
+    const long long total = (long long) M * N * P;
+    const int nV = axis == 0 ? M : axis == 1 ? N : P;
+    const long long stride = axis == 0 ? 1 : axis == 1 ? (long long) M : (long long) M * N;
+    const int nK = K.n, k2 = (nK - 1) / 2;
+    for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < total;
+         e += (long long) gridDim.x * blockDim.x) {
+        const int a = (int) (e % M);
+        const int b = (int) ((e / M) % N);
+        const int c = (int) (e / ((long long) M * N));
+        const int v = axis == 0 ? a : axis == 1 ? b : c;
+        const float *line = in + (e - (long long) v * stride);  // element 0 of this line
+        double acc = 0.0, kacc = 0.0;
+        float r;
+        if (nK > nV) {
+            const int from = v > k2 ? v - k2 : 0;
+            const int to = v + k2 + 1 > nV ? nV : v + k2 + 1;
+            for (int l = from; l < to; ++l) {
+                acc += (double) __fmul_rn(line[l * stride], K.k[l - v + k2]);
+                kacc += (double) K.k[l - v + k2];
+            }
+            r = (float) (acc / kacc);
+        } else if (v < k2) {
+            for (int kk = k2 - v; kk < nK; ++kk) {
+                acc += (double) __fmul_rn(K.k[kk], line[(v - k2 + kk) * stride]);
+                kacc += (double) K.k[kk];
+            }
+            r = (float) (acc / kacc);
+        } else if (v + k2 < nV) {
+            for (int kk = 0; kk < nK; ++kk) acc += (double) __fmul_rn(K.k[kk], line[(v - k2 + kk) * stride]);
+            r = (float) acc;
+        } else {
+            for (int kk = 0; kk < nV - v + k2; ++kk) {
+                acc += (double) __fmul_rn(K.k[kk], line[(v - k2 + kk) * stride]);
+                kacc += (double) K.k[kk];
+            }
+            r = (float) (acc / kacc);
+        }
+        out[e] = r;
+    }
+}
+
 // fim_subregion (fim.c:695-718): the image-sized corner of a job volume
 __global__ void k_crop(const float *__restrict__ x, int X, int Y, int M, int N, int P, float *__restrict__ out)
 {

@@ -225,6 +225,97 @@ static float get_error(job_t *J, const float *y, const float *im, int metric)
 
 /* ------------------------------------------------------------ driver */
 
+/* gaussian_kernel, src/fim.c:2077-2106 (normalised to sum 1) */
+static float *gauss_kernel(float sigma, size_t *nK)
+{
+    int len = (int) ceil(3.0 * sigma);
+    if (len < 1) len = 1;
+    int n = 2 * len + 1;
+    float *K = malloc(sizeof(float) * (size_t) n);
+    float mid = (n - 1) / 2;
+    float s2 = pow(sigma, 2);
+    float k0 = 1.0 / sigma / sqrt(2.0 * M_PI);
+    double sum = 0;
+    for (int kk = 0; kk < n; kk++) {
+        float x = (float) kk - mid;
+        K[kk] = k0 * exp(-0.5 * pow(x, 2) / s2);
+        sum += K[kk];
+    }
+    for (int kk = 0; kk < n; kk++) K[kk] /= sum;
+    *nK = (size_t) n;
+    return K;
+}
+
+/* fim_conv1_vector with normalized = 1, src/fim.c:1944-2066: products in
+ * float, sums in double, kernel renormalised where it leaves the line */
+static void conv1_norm(float *V, size_t stride, float *W, size_t nV, const float *K, size_t nK)
+{
+    const size_t k2 = (nK - 1) / 2;
+    size_t b = 0;
+    if (nK > nV) {
+        for (size_t kk = 0; kk < nV; kk++) {
+            double acc0 = 0, kacc = 0;
+            size_t from = k2 > kk ? 0 : kk - k2;
+            size_t to = kk + k2 + 1 > nV ? nV : kk + k2 + 1;
+            for (size_t ll = from; ll < to; ll++) {
+                acc0 += V[ll * stride] * K[ll - kk + k2];
+                kacc += K[ll - kk + k2];
+            }
+            W[kk] = acc0 / kacc;
+        }
+    } else {
+        for (size_t vv = 0; vv < k2; vv++) {
+            double acc0 = 0, kacc = 0;
+            for (size_t kk = k2 - vv; kk < nK; kk++) {
+                acc0 = acc0 + K[kk] * V[(vv - k2 + kk) * stride];
+                kacc += K[kk];
+            }
+            W[b++] = acc0 / kacc;
+        }
+        for (size_t vv = k2; vv + k2 < nV; vv++) {
+            double acc = 0;
+            for (size_t kk = 0; kk < nK; kk++) acc = acc + K[kk] * V[((vv - k2) + kk) * stride];
+            W[b++] = acc;
+        }
+        for (size_t vv = nV - k2; vv < nV; vv++) {
+            double kacc = 0, acc0 = 0;
+            for (size_t kk = 0; kk < nV - vv + k2; kk++) {
+                acc0 = acc0 + K[kk] * V[(vv - k2 + kk) * stride];
+                kacc += K[kk];
+            }
+            W[b++] = acc0 / kacc;
+        }
+    }
+    for (size_t p = 0; p < nV; p++) V[p * stride] = W[p];
+}
+
+/* fim_gsmooth(V, M, N, P, sigma) = fim_gsmooth_aniso(V, ..., sigma, sigma),
+ * src/fim.c:2240-2278: x, then y, then z with the kernel trimmed to at most
+ * 2P-1 taps (z only when P > 1) */
+void dwo_gsmooth(float *V, i64 M, i64 N, i64 P, float sigma)
+{
+    size_t nK = 0;
+    float *K = gauss_kernel(sigma, &nK);
+    size_t nb = (size_t) (M > N ? (M > P ? M : P) : (N > P ? N : P));
+    float *W = malloc(sizeof(float) * nb);
+    for (i64 pp = 0; pp < P; pp++)
+        for (i64 nn = 0; nn < N; nn++) conv1_norm(V + pp * M * N + nn * M, 1, W, (size_t) M, K, nK);
+    for (i64 pp = 0; pp < P; pp++)
+        for (i64 mm = 0; mm < M; mm++) conv1_norm(V + pp * M * N + mm, (size_t) M, W, (size_t) N, K, nK);
+    if (P > 1) {
+        const float *Ka = K;
+        size_t nKa = nK;
+        while (nKa > (size_t) (2 * P - 1)) {
+            Ka++;
+            nKa -= 2;
+        }
+        for (i64 nn = 0; nn < N; nn++)
+            for (i64 mm = 0; mm < M; mm++) conv1_norm(V + mm + M * nn, (size_t) (M * N), W, (size_t) P, Ka, nKa);
+    }
+    free(W);
+    free(K);
+}
+
 int dwo_deconvolve(const float *im, i64 M, i64 N, i64 P,
                    const float *psf, i64 pM, i64 pN, i64 pP,
                    dwo_opts *s, float *out)
@@ -239,7 +330,6 @@ int dwo_deconvolve(const float *im, i64 M, i64 N, i64 P,
         memcpy(out, im, sizeof(float) * MNP);
         return 0;
     }
-    if (s->start_condition == 1) return -2; /* LP start is not restated */
 
     /* method_shb.c:108-117: bg = max(min(im), 0.01) */
     if (s->bg_auto) {
@@ -321,10 +411,21 @@ int dwo_deconvolve(const float *im, i64 M, i64 N, i64 P,
         float v = sumg / (float) wMNP_logical;
         for (size_t k = 0; k < wMNP; k++) x[k] = v;
     } else {
+        /* IDENTITY: the image; LP (method_shb.c:278-285): the image smoothed
+         * by fim_gsmooth with sigma 8; both inserted at the corner */
+        const float *src = im;
+        float *lp = NULL;
+        if (s->start_condition == 1) {
+            lp = malloc(sizeof(float) * MNP);
+            memcpy(lp, im, sizeof(float) * MNP);
+            dwo_gsmooth(lp, M, N, P, 8);
+            src = lp;
+        }
         memset(x, 0, sizeof(float) * wMNP);
         for (i64 c = 0; c < P; c++)
             for (i64 b = 0; b < N; b++)
-                for (i64 a = 0; a < M; a++) x[a + wM * b + wM * wN * c] = im[a + M * b + M * N * c];
+                for (i64 a = 0; a < M; a++) x[a + wM * b + wM * wN * c] = src[a + M * b + M * N * c];
+        free(lp);
     }
     memcpy(xp, x, sizeof(float) * wMNP);
 

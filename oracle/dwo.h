@@ -27,7 +27,7 @@ typedef struct dwo_opts {
     int32_t bg_auto;
     int32_t positivity;
     int32_t border_quality;  /* bq: 0, 1, 2 */
-    int32_t start_condition; /* 0 FLAT, 1 LP (not restated), 2 IDENTITY */
+    int32_t start_condition; /* 0 FLAT, 1 LP (Gaussian low-pass, sigma 8), 2 IDENTITY */
     int32_t metric;          /* 0 MSE, 1 IDIV */
     float alphamax;
     int32_t threads;         /* OpenMP threads, <= 0: default */
@@ -58,6 +58,9 @@ void dwo_circshift(float *A, int64_t M, int64_t N, int64_t P,
                    int64_t sm, int64_t sn, int64_t sp);
 float dwo_idiv(const float *y, const float *g, int64_t M, int64_t N, int64_t P,
                int64_t wM, int64_t wN, int64_t wP);
+
+/* fim_gsmooth (in place, M x N x P). */
+void dwo_gsmooth(float *V, int64_t M, int64_t N, int64_t P, float sigma);
 
 /* PSF preparation and tiling (dwo.c cites the reference lines). */
 float *dwo_psf_autocrop(float *psf, int64_t *pM, int64_t *pN, int64_t *pP, int64_t M, int64_t N, int64_t P,

@@ -183,3 +183,17 @@ def test_port_reproduces_golden(name):
     assert r.iterations == int(d["iterations"])
     np.testing.assert_array_equal(r.trace, d["trace"])
     np.testing.assert_array_equal(r.out, d["out"])
+
+
+@pytest.mark.skipif(not po.available("reference"), reason="oracle/_ref not built")
+@pytest.mark.parametrize("shape", [(9, 22, 19), (1, 30, 26), (3, 60, 70), (40, 20, 56)])
+@pytest.mark.parametrize("method", ["shb", "rl"])
+def test_lp_start_port_equals_reference(shape, method):
+    """The low-pass start (fim_gsmooth with sigma 8, fim.c:2240-2278) as
+    restated in the port equals the reference's own, bit for bit."""
+    psf = gauss_psf((3, 5, 5) if shape[0] < 5 else (5, 7, 9), (1.2, 1.5, 1.7), seed=2, jitter=0.2)
+    im = poisson_image(shape, psf, seed=2, bg=50.0, npts=12)
+    a = po.deconvolve(im, psf, method=method, n_iter=3, start=po.START_LP)
+    b = po.deconvolve(im, psf, method=method, n_iter=3, start=po.START_LP, impl="reference")
+    np.testing.assert_array_equal(a.out, b.out)
+    np.testing.assert_array_equal(a.trace, b.trace)
