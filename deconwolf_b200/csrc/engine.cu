@@ -180,6 +180,14 @@ struct Geometry {
     const XPlan *xp;
     const LinesPlan *yp, *zp;
     const YPlan *ytp;       // pipelined y pass when the tile fits shared memory
+    // Periodic axes: with border_quality 0 or 1 the reference convolves
+    // circularly with period w.  An axis whose exact length w has no
+    // supported transform is transformed at a length >= w + 2h instead: the
+    // fields live on [0, w), the margins [w, w+h) and [len-h, len) hold
+    // copies of [0, h) and [w-h, w), so the linear convolution by the PSF
+    // (half-width h about its centre) equals the circular one on [0, w).
+    bool wx = false, wy = false, wz = false;
+    long long hx = 0, hy = 0, hz = 0;
     long long spec_elems() const { return Z * NKB * Y * KB; }
     long long real_elems() const { return XP * Y * Z; }
 };
@@ -213,10 +221,14 @@ static int make_geometry(long long M, long long N, long long P, long long pM, lo
     g.X = pad_x(g.wM, exact);
     g.Y = pad_lines(g.wN, exact);
     g.Z = pad_lines(g.wP, exact);
+    if (exact) {
+        // axes without a transform of the exact length: periodic margins
+        if (g.X < 0) { g.wx = true; g.hx = (pM - 1) / 2; g.X = pad_x(g.wM + 2 * g.hx, false); }
+        if (g.Y < 0) { g.wy = true; g.hy = (pN - 1) / 2; g.Y = pad_lines(g.wN + 2 * g.hy, false); }
+        if (g.Z < 0) { g.wz = true; g.hz = (pP - 1) / 2; g.Z = pad_lines(g.wP + 2 * g.hz, false); }
+    }
     if (g.X < 0 || g.Y < 0 || g.Z < 0)
-        return fail(DWCU_ERROR_UNSUPPORTED,
-                    "no supported FFT size for job %lld x %lld x %lld (border_quality %d needs exact "
-                    "7-smooth sizes with three radices <= 16; x must be even)",
+        return fail(DWCU_ERROR_UNSUPPORTED, "no supported FFT size for job %lld x %lld x %lld (border_quality %d)",
                     g.wM, g.wN, g.wP, bq);
     g.xp = find_x((int) (g.X / 2));
     g.yp = g.Y > 1 ? find_lines((int) g.Y) : nullptr;
@@ -594,6 +606,11 @@ static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, con
     a.rl_clamp = 1;
     a.alpha = alpha;
     a.alpha_next = alpha_next;
+    // the OTF is the shifted PSF, not a periodic field: no margins
+    const bool wrap = S != j->K;
+    a.wrapx = (wrap && g.wx) ? 1 : 0;
+    a.wM = (int) g.wM;
+    a.hx = (int) g.hx;
     // algorithmic traffic of this launch
     static const char *names[] = {"x_fwd_copy", "x_fwd_ones", "x_fwd_shbp", "x_ratio_shb", "x_ratio_rl",
                                   "x_error", "x_update_shb", "x_update_rl", "x_weights", "x_store"};
@@ -617,6 +634,14 @@ static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, con
     ProfScope ps(names[op], bytes, j->stream);
     g.xp->launch(a, j->stream);
     CHECK_LAUNCH();
+    if (r2c && wrap && (g.wy || g.wz)) {
+        // periodic y/z: margin rows of the new spectrum copy the rows they wrap to
+        const long long segs = g.Z * g.NKB * g.Y;
+        const int blocks = (int) std::min<long long>(148 * 16, (segs + 255) / 256);
+        k_wrap_rows<<<blocks, 256, 0, j->stream>>>(S, (int) g.Y, (int) g.Z, (int) g.NKB, (int) g.wN, (int) g.hy,
+                                                   g.wy ? 1 : 0, (int) g.wP, (int) g.hz, g.wz ? 1 : 0);
+        CHECK_LAUNCH();
+    }
     return DWCU_SUCCESS;
 }
 
@@ -669,7 +694,8 @@ static int conv_forward(dwcu_job *j)
 static int conv_backward(dwcu_job *j)
 {
     const Geometry &g = j->g;
-    if (j->s.method != DWCU_METHOD_SHB) return conv(j, 1);
+    // (a periodic z copies image planes into its margins: no zero planes)
+    if (j->s.method != DWCU_METHOD_SHB || g.wz) return conv(j, 1);
     TRY(pass_y(j, LINES_FWD, j->S, g.P));
     TRY(pass_z(j, LINES_CONV_CONJ, j->S, g.P, g.Z));
     TRY(pass_y(j, LINES_INV, j->S));
@@ -686,7 +712,8 @@ static int iter_forward(dwcu_job *j, int k, bool ratio)
     TRY(conv_forward(j));
     int op = ratio ? (shb ? XOP_RATIO_SHB : XOP_RATIO_RL) : XOP_ERROR_ONLY;
     const long long ytiles = (g.Y + g.xp->R - 1) / g.xp->R;
-    const long long tiles = (op == XOP_RATIO_RL) ? j->nxb : g.P * ytiles;
+    // planes z >= P are read later by RL, and by a periodic z (its margins)
+    const long long tiles = (op == XOP_RATIO_RL || g.wz) ? j->nxb : g.P * ytiles;
     TRY(pass_x(j, op, ratio ? 1 : 0, j->S, nullptr, nullptr, nullptr, 0, 0, tiles));
     TRY(err_final(j, k, tiles));
     return DWCU_SUCCESS;
@@ -851,6 +878,19 @@ static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_dev
     CHECK_LAUNCH();
     k_argmax_final<<<1, 32, 0, st>>>(j->apart, nab, j->amax);
     CHECK_LAUNCH();
+    if (g.wx || g.wy || g.wz) {
+        // the periodic margins assume the PSF maximum within h of both ends
+        long long am = 0;
+        CU(cudaMemcpyAsync(&am, j->amax, sizeof am, cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        const long long ax = am % g.pM, ay = (am / g.pM) % g.pN, az = am / (g.pM * g.pN);
+        auto off = [](long long a, long long p) { return std::max(a, p - 1 - a); };
+        if ((g.wx && off(ax, g.pM) > g.hx) || (g.wy && off(ay, g.pN) > g.hy) || (g.wz && off(az, g.pP) > g.hz))
+            return fail(DWCU_ERROR_UNSUPPORTED,
+                        "border_quality %d with a job size that has no exact transform needs the PSF maximum at "
+                        "its centre (maximum at %lld, %lld, %lld of %lld x %lld x %lld)",
+                        j->s.border_quality, ax, ay, az, g.pM, g.pN, g.pP);
+    }
     const size_t R = sizeof(float) * (size_t) g.real_elems();
     CU(cudaMemsetAsync(j->S, 0, sizeof(float2) * (size_t) g.spec_elems(), st));
     CU(cudaMemsetAsync(j->K, 0, sizeof(float2) * (size_t) g.spec_elems(), st));

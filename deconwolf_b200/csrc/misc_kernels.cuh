@@ -252,6 +252,38 @@ __global__ void k_gsmooth_axis(const float *__restrict__ in, float *__restrict__
     }
 }
 
+// Periodic y and/or z (bq 0/1 axes transformed at a larger length): after a
+// forward x pass, every spectrum row (y, z) outside [0, wN) x [0, wP) takes
+// a copy of the row it wraps to -- [w, w+h) from [0, h), [len-h, len) from
+// [w-h, w) -- and the rows in between are cleared.  One thread per 4-wide
+// kx block of a row.
+__global__ void k_wrap_rows(float2 *__restrict__ S, int Y, int Z, int nkb, int wN, int hy, int wrapy, int wP, int hz,
+                            int wrapz)
+{
+    const long long n = (long long) Z * nkb * Y;
+    for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < n;
+         e += (long long) gridDim.x * blockDim.x) {
+        const int y = (int) (e % Y);
+        const long long zk = e / Y;
+        const int kb = (int) (zk % nkb);
+        const int z = (int) (zk / nkb);
+        const bool yin = !wrapy || y < wN, zin = !wrapz || z < wP;
+        if (yin && zin) continue;
+        auto src = [](int v, int w, int h, int len) { return v < w ? v : v < w + h ? v - w : v >= len - h ? v - len + w : -1; };
+        const int ys = wrapy ? src(y, wN, hy, Y) : y;
+        const int zs = wrapz ? src(z, wP, hz, Z) : z;
+        float2 *dst = S + (((long long) z * nkb + kb) * Y + y) * KB;
+        if (ys < 0 || zs < 0) {
+#pragma unroll
+            for (int i = 0; i < KB; ++i) dst[i] = make_float2(0.f, 0.f);
+        } else {
+            const float2 *from = S + (((long long) zs * nkb + kb) * Y + ys) * KB;
+#pragma unroll
+            for (int i = 0; i < KB; ++i) dst[i] = from[i];
+        }
+    }
+}
+
 // fim_subregion (fim.c:695-718): the image-sized corner of a job volume
 __global__ void k_crop(const float *__restrict__ x, int X, int Y, int M, int N, int P, float *__restrict__ out)
 {

@@ -417,6 +417,10 @@ struct XArgs {
     int rl_clamp;          // RL: clamp x' at bg when bg > 0
     double alpha;          // SHB extrapolation weight of the step being finished
     double alpha_next;     // SHB extrapolation weight of the next step
+    // periodic x (wrapx): the row is wM-periodic; before the forward
+    // transform, [wM, wM+hx) and [X-hx, X) take copies of [0, hx) and
+    // [wM-hx, wM), the rest of [wM, X) is zero
+    int wrapx, wM, hx;
 };
 
 // The x transform of a real row of X = 2L samples uses a complex transform
@@ -708,7 +712,9 @@ k_xpass(XArgs a)
     const int y0 = (tile - z * ytiles) * R;
 
     if constexpr (FAM == XFAM_RATIO) {
-        if (z >= a.P || y0 >= a.N) {
+        // (with a periodic x, RL's constant row is not constant over the
+        // transform length: such rows take the general path)
+        if ((z >= a.P || y0 >= a.N) && !(a.wrapx && op == XOP_RATIO_RL)) {
             // No image row in this tile: the ratio is the same constant on
             // every row (0 for SHB, method_shb.c:44-46; 1e-6 for RL,
             // method_rl.c:62-64) and the rows add nothing to the error, so
@@ -847,6 +853,43 @@ k_xpass(XArgs a)
 
     // ---- forward with the reversed radix list; w is its first-stage input
     __syncthreads();  // all reads of the exchange tiles are complete
+    if (a.wrapx) {
+        // periodic margins of the row (see XArgs), through shared memory
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            float *rowf = reinterpret_cast<float *>(smem(q, 0));
+            if (t < SL) {
+#pragma unroll
+                for (int r = 0; r < RD::RL; ++r) {
+                    const int n = t + r * SL;
+                    rowf[2 * n] = w[q][r].x;
+                    rowf[2 * n + 1] = w[q][r].y;
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float *rowf = reinterpret_cast<const float *>(smem(q, 0));
+            if (t < SL) {
+#pragma unroll
+                for (int r = 0; r < RD::RL; ++r) {
+                    const int n = t + r * SL;
+                    float e[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int c = 2 * n + h;
+                        const int src = c < a.wM ? c
+                                      : c < a.wM + a.hx ? c - a.wM
+                                      : c >= C::X - a.hx ? c - C::X + a.wM : -1;
+                        e[h] = src >= 0 ? rowf[src] : 0.f;
+                    }
+                    w[q][r] = make_float2(e[0], e[1]);
+                }
+            }
+        }
+        __syncthreads();
+    }
     float2 qo[Q][RV::RL];
     line_fft<RV, -1, Q, PREF_TW>(w, qo, t, a.twL, smem);
     constexpr int SQ = L / RV::RL;

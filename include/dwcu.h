@@ -37,7 +37,7 @@ extern "C" {
 typedef enum dwcu_status {
     DWCU_SUCCESS = 0,
     DWCU_ERROR_INVALID_VALUE = 1, /* bad argument (sizes, null pointers, options) */
-    DWCU_ERROR_UNSUPPORTED = 2,   /* valid for deconwolf, not implemented here (e.g. an exact bq 0/1 size with a prime factor > 7) */
+    DWCU_ERROR_UNSUPPORTED = 2,   /* valid for deconwolf, not implemented here (e.g. a job longer than the longest transform, or bq 0/1 periodic margins with an off-centre PSF maximum) */
     DWCU_ERROR_OUT_OF_MEMORY = 3, /* device allocation failed or HBM budget exceeded */
     DWCU_ERROR_CUDA = 4,          /* CUDA runtime / launch failure, or no device */
     DWCU_ERROR_INPUT = 5,         /* non-finite image or PSF values */
@@ -64,7 +64,7 @@ typedef struct dwcu_opts {
     float bg;                /* background; overwritten when bg_auto          (dw_opts.bg) */
     int32_t bg_auto;         /* 1: bg = max(min(image), 0.01), default 1       (dw_opts.bg_auto) */
     int32_t positivity;      /* SHB: clamp the estimate at bg, default 1      (dw_opts.positivity) */
-    int32_t border_quality;  /* 2 (default); 1 and 0 need exact-size FFTs    (dw_opts.borderQuality) */
+    int32_t border_quality;  /* 2 (default); 1 and 0 convolve periodically    (dw_opts.borderQuality) */
     int32_t start_condition; /* FLAT (default), IDENTITY or LP (sigma 8)      (dw_opts.start_condition) */
     int32_t metric;          /* IDIV (default) or MSE                         (dw_opts.metric) */
     float alphamax;          /* SHB extrapolation cap, default 1              (dw_opts.alphamax) */

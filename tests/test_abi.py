@@ -51,21 +51,27 @@ def test_plan_sizes_of_the_workloads():
 
 
 def test_exact_sizes_for_bq_0_and_1():
-    # bq 1/0 wrap around inside the job, so only exact supported sizes work:
+    # bq 1/0 wrap around inside the job: exact sizes where supported,
     # 256 + 64 = 320 (x, 160 = 16*10), 256 + 64 = 320, 40 + 40 = 80
     assert dw.plan_size((40, 256, 256), (79, 127, 127), border_quality=1)[0] == (320, 320, 80)
-    # bq 0: max(M, pM): 13 is prime -> not a supported exact size
-    with pytest.raises(dw.DwcuError) as e:
-        dw.plan_size((13, 64, 64), (5, 5, 5), border_quality=0)
-    assert e.value.code == 2
+    # bq 0: max(M, pM): z period 13 is prime -> periodic z at the next
+    # supported length >= 13 + 2*2
+    assert dw.plan_size((13, 64, 64), (5, 5, 5), border_quality=0)[0] == (64, 64, 18)
 
 
 def test_bq1_exact_supported_size():
     # M + (pM+1)/2 = 60 + 4 = 64 (x), 50 + 4 = 54, 20 + 4 = 24: all supported and exact
     work, _ = dw.plan_size((20, 50, 60), (7, 7, 7), border_quality=1)
     assert work == (64, 54, 24)
+    # 61 + 4 = 65 is odd: x is transformed at a length >= 65 + 2*3 with
+    # periodic margins (72); y and z stay exact
+    work, _ = dw.plan_size((20, 50, 61), (7, 7, 7), border_quality=1)
+    assert work == (72, 54, 24)
+    # bq 0 with a prime z period: 37 + 2*5 -> the next supported length
+    work, _ = dw.plan_size((37, 40, 30), (11, 9, 9), border_quality=0)
+    assert work[:2] == (30, 40) and work[2] >= 37 + 2 * 5
     with pytest.raises(dw.DwcuError) as e:
-        dw.plan_size((20, 50, 61), (7, 7, 7), border_quality=1)  # 65 is odd
+        dw.plan_size((1, 1, 5000), (1, 1, 3))  # beyond the longest x transform
     assert e.value.code == 2
 
 

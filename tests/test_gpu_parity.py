@@ -89,6 +89,31 @@ def test_shapes_and_border_quality(shape, psf_shape, bq):
         assert trace_err(g.trace, r.trace) < TRACE_TOL, m
 
 
+PERIODIC = [
+    ((9, 22, 20), (5, 7, 9), 1),     # bq 1: x 25 (odd) and y 26 periodic, z 12 exact
+    ((37, 40, 30), (11, 9, 9), 0),   # bq 0: z period 37 (prime)
+    ((20, 33, 44), (21, 15, 13), 0), # bq 0: x 44 (22 = 2*11) and y 33 periodic, z 21 exact
+    ((12, 26, 31), (7, 9, 11), 1),   # bq 1: every axis periodic (37, 31, 16 -> x odd, y prime)
+]
+
+
+@pytest.mark.parametrize("shape,psf_shape,bq", PERIODIC)
+@pytest.mark.parametrize("kw", [dict(method="shb", n_iter=10), dict(method="rl", n_iter=8),
+                                dict(method="shb", iter_type=po.ITER_REL, err_rel=0.005)],
+                         ids=["shb", "rl", "shb-rel"])
+def test_periodic_sizes_match_reference(shape, psf_shape, bq, kw):
+    """border_quality 0/1 at job sizes without an exact transform: the
+    circular convolution of the reference's job size is carried out at a
+    longer length with periodic margins; against the reference at its own
+    (exact) size."""
+    im, psf = case_inputs(seed=6, shape=shape, psf_shape=psf_shape)
+    g = dw.run_method(im, psf, border_quality=bq, **kw)
+    r = po.deconvolve(im, psf, border_quality=bq, impl=checker(), **kw)
+    assert g.iterations == r.iterations
+    assert rel_l2(g.out, r.out) < OUT_TOL
+    assert trace_err(g.trace, r.trace) < TRACE_TOL
+
+
 def test_identity_and_first_iteration():
     im, psf = case_inputs()
     np.testing.assert_array_equal(dw.run_method(im, psf, n_iter=0).out, im)
@@ -189,8 +214,14 @@ def test_input_errors():
         dw.run_method(bad, psf, n_iter=3)
     assert e.value.code == 5
     with pytest.raises(dw.DwcuError) as e:
-        # bq 1 needs the exact job size: x = 20 + (9 + 1) / 2 = 25 is odd
-        dw.run_method(im[:, :, :20].copy(), psf, n_iter=3, border_quality=1)
+        # beyond the longest supported x transform
+        dw.run_method(np.full((1, 1, 5000), 50, np.float32), np.full((1, 1, 3), 1 / 3, np.float32), n_iter=3)
+    assert e.value.code == 2
+    with pytest.raises(dw.DwcuError) as e:
+        # periodic margins need the PSF maximum at its centre
+        off = psf.copy()
+        off[0, 0, 0] = off.max() * 2
+        dw.run_method(im[:, :, :20].copy(), off, n_iter=3, border_quality=1)
     assert e.value.code == 2
     # the context is still usable afterwards
     assert dw.run_method(im, psf, n_iter=2).iterations == 2
