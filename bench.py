@@ -214,6 +214,20 @@ def _common_line(metric, value, args, config, extra):
     return line
 
 
+_PINNED = []
+
+
+def _pinned(a=None, shape=None):
+    """A numpy view of page-locked host memory: a copy of ``a``, or an
+    uninitialised float32 array of ``shape`` (the host buffers of the
+    end-to-end measurements)."""
+    import torch
+    t = (torch.from_numpy(np.ascontiguousarray(a)).pin_memory() if a is not None
+         else torch.empty(shape, dtype=torch.float32, pin_memory=True))
+    _PINNED.append(t)
+    return t.numpy()
+
+
 def run_tiles(args):
     import deconwolf_b200 as dw
     from deconwolf_b200 import synthetic
@@ -222,9 +236,12 @@ def run_tiles(args):
     log(f"inputs {im.shape} in {time.time() - t0:.1f}s")
     pp = dw.psf_prepare(psf, im.shape)
     tiles = dw.tiling_create(im.shape, args.tilesize, 50)
+    im = _pinned(im)
+    outs = {0.0: _pinned(shape=im.shape), 1.0: _pinned(shape=im.shape)}
 
     def step(budget=0.0):
-        return dw.deconvolve_tiled(im, pp, args.tilesize, 50, method="shb", n_iter=ITERS, hbm_budget=budget)
+        return dw.deconvolve_tiled(im, pp, args.tilesize, 50, method="shb", n_iter=ITERS, hbm_budget=budget,
+                                   out=outs[budget])
 
     for _ in range(args.warmup):
         step()
@@ -240,7 +257,8 @@ def run_tiles(args):
     print(json.dumps(_common_line(
         f"Mvoxel*iter/s (SHB, tiled {M}x{N}x{P})", vox_it / dt / 1e6, args,
         {"workload": "tiles-4096x4096x60", "image": [M, N, P], "psf": list(psf.shape[::-1]),
-         "tilesize": args.tilesize, "overlap": 50, "tiles": len(tiles), "iterations": ITERS, "method": "shb"},
+         "tilesize": args.tilesize, "overlap": 50, "tiles": len(tiles), "iterations": ITERS, "method": "shb",
+         "host_buffers": "page-locked image and result"},
         {"ms_per_step": dt * 1e3,
          "sequential": {"value": vox_it / dt_seq / 1e6, "ms_per_step": dt_seq * 1e3,
                         "how": "dwcu_deconvolve_tiled with one tile per batch"},
@@ -256,8 +274,10 @@ def run_channels(args):
     for c in range(6):
         im, psf = synthetic.channel_inputs(c, CACHE)
         sp = synthetic.channel_spec(c)
-        chans.append((im, dw.psf_prepare(psf, im.shape), sp["iters"]))
+        chans.append((_pinned(im), dw.psf_prepare(psf, im.shape), sp["iters"]))
     log(f"6 channels in {time.time() - t0:.1f}s: " + ", ".join(str(c[0].shape) for c in chans))
+    outs_b = [_pinned(shape=c[0].shape) for c in chans]
+    outs_s = [_pinned(shape=c[0].shape) for c in chans]
 
     def batched():
         jobs = []
@@ -266,13 +286,13 @@ def run_channels(args):
             j.setup(im, p)
             jobs.append(j)
         dw.batch_run(jobs)
-        outs = [j.result() for j in jobs]
+        outs = [j.result(out=o) for j, o in zip(jobs, outs_b)]
         for j in jobs:
             j.close()
         return outs
 
     def sequential():
-        return [dw.run_method(im, p, method="shb", n_iter=it) for im, p, it in chans]
+        return [dw.run_method(im, p, out=o, method="shb", n_iter=it) for (im, p, it), o in zip(chans, outs_s)]
 
     for _ in range(args.warmup):
         batched()
@@ -289,7 +309,8 @@ def run_channels(args):
     print(json.dumps(_common_line(
         "Mvoxel*iter/s (SHB, 6-channel field of view)", vox_it / dt / 1e6, args,
         {"workload": "channels-6", "channels": [{"image": list(im.shape[::-1]), "psf": list(p.shape[::-1]),
-                                                 "iterations": it} for im, p, it in chans], "method": "shb"},
+                                                 "iterations": it} for im, p, it in chans], "method": "shb",
+         "host_buffers": "page-locked images and results"},
         {"ms_per_step": dt * 1e3,
          "sequential": {"value": vox_it / dt_seq / 1e6, "ms_per_step": dt_seq * 1e3,
                         "how": "dwcu_deconvolve per channel, one after another"},
@@ -376,6 +397,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=[WORKLOAD, SMALL, PROFILE_CASE, "shb-2048x256x20", "shb-256x2048x20", "shb-256x256x60",
+                             "shb-1124x1124x60",
                              "tiles-4096x4096x60", "channels-6", "serve-stream"])
     ap.add_argument("--tilesize", type=int, default=1024)
     ap.add_argument("--requests", type=int, default=60, help="serve-stream: number of requests (full stream: 500)")

@@ -125,7 +125,7 @@ EXPORTS = [
     "dwcu_profile_enable", "dwcu_profile_collect", "dwcu_batch_run", "dwcu_psf_prepare",
     "dwcu_tiling_create", "dwcu_deconvolve_tiled", "dwcu_fft_r2c_noalloc", "dwcu_server_create",
     "dwcu_server_submit", "dwcu_server_wait", "dwcu_server_cancel", "dwcu_server_get_stats",
-    "dwcu_server_destroy", "dwcu_tile_blend",
+    "dwcu_server_destroy", "dwcu_tile_blend", "dwcu_release_cache",
 ]
 
 _lib = None
@@ -150,6 +150,8 @@ def lib() -> ctypes.CDLL:
     L.dwcu_deconvolve_device.restype = ctypes.c_int
     L.dwcu_plan_size.argtypes = [i64, i64, i64, i64, i64, i64, i32, i32, ctypes.POINTER(i64), ctypes.POINTER(i64)]
     L.dwcu_plan_size.restype = ctypes.c_int
+    L.dwcu_release_cache.argtypes = [i32]
+    L.dwcu_release_cache.restype = ctypes.c_int
     L.dwcu_job_create.argtypes = [i64, i64, i64, i64, i64, i64, P_opts, ctypes.POINTER(vp)]
     L.dwcu_job_create.restype = ctypes.c_int
     L.dwcu_job_setup.argtypes = [vp, vp, vp, i32]
@@ -251,9 +253,11 @@ class Result:
         self.seconds_enqueue = o.seconds_enqueue
 
 
-def run_method(im: np.ndarray, psf: np.ndarray, **kw) -> Result:
+def run_method(im: np.ndarray, psf: np.ndarray, out: np.ndarray | None = None, **kw) -> Result:
     """The dw_function call on host arrays: ``im`` (P, N, M) and ``psf``
-    (pP, pN, pM), float32, x fastest.  Keyword options as :func:`make_opts`."""
+    (pP, pN, pM), float32, x fastest.  Keyword options as :func:`make_opts`.
+    ``out``: an optional C-contiguous float32 array of the image's shape for
+    the result (for example in page-locked memory)."""
     im = np.ascontiguousarray(im, dtype=np.float32)
     psf = np.ascontiguousarray(psf, dtype=np.float32)
     if im.ndim != 3 or psf.ndim != 3:
@@ -263,12 +267,26 @@ def run_method(im: np.ndarray, psf: np.ndarray, **kw) -> Result:
     trace = np.zeros(cap, dtype=np.float32)
     o.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     o.trace_capacity = cap
-    out = np.empty_like(im)
+    out = _out_array(out, im.shape)
     P, N, M = im.shape
     pP, pN, pM = psf.shape
     _check(lib().dwcu_deconvolve(im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP,
                                  ctypes.byref(o), out.ctypes.data))
     return Result(out, trace[: o.iterations_done].copy(), o)
+
+
+def release_cache(device: int = -1) -> None:
+    """Free the device blocks kept for reuse by later jobs
+    (dwcu_release_cache); ``device`` < 0: every device."""
+    _check(lib().dwcu_release_cache(device))
+
+
+def _out_array(out, shape):
+    if out is None:
+        return np.empty(shape, dtype=np.float32)
+    if out.shape != tuple(shape) or out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
+        raise ValueError(f"out must be a C-contiguous float32 array of shape {tuple(shape)}")
+    return out
 
 
 def run_method_device(d_im, d_psf, d_out, shape, psf_shape, stream: int = 0, **kw) -> Result:
@@ -345,13 +363,14 @@ def tiling_create(shape, max_size: int, overlap: int = 20) -> list[dict]:
 
 def deconvolve_tiled(im: np.ndarray, psf: np.ndarray, tile_size: int, overlap: int = 20,
                      offset: float = 5.0, xycropfactor: float = 0.001, hbm_budget: float = 0.0,
-                     **kw) -> Result:
+                     out: np.ndarray | None = None, **kw) -> Result:
     """deconvolve_tiles (dw.c:2001-2229) on host arrays; ``psf`` as dw_run
-    hands it over (already prepared for the whole image)."""
+    hands it over (already prepared for the whole image).  ``out`` as for
+    :func:`run_method`."""
     im = np.ascontiguousarray(im, dtype=np.float32)
     psf = np.ascontiguousarray(psf, dtype=np.float32)
     o = make_opts(**kw)
-    out = np.empty_like(im)
+    out = _out_array(out, im.shape)
     P, N, M = im.shape
     pP, pN, pM = psf.shape
     _check(lib().dwcu_deconvolve_tiled(im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP, tile_size,

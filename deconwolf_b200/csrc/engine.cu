@@ -22,6 +22,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dwcu.h"
@@ -327,9 +328,10 @@ static int get_twiddles(DeviceCtx *c, long long n, const float2 **out)
 // ------------------------------------------------------------ memory blocks
 //
 // A job's device memory is one block.  Released blocks are kept per device
-// (a few at most) and handed to the next job of the same size, so a stream of
-// equal-sized jobs (tiles, repeated deconvolutions) allocates once; the
-// iteration graphs captured on a block stay valid with it and are reused.
+// (a few at most) and handed to the next job that fits and needs at least
+// four fifths of the block, so a stream of similar-sized jobs (tiles,
+// repeated deconvolutions) allocates once; the iteration graphs captured on
+// a block stay valid with it and are reused.
 
 struct Block {
     char *ptr = nullptr;
@@ -345,7 +347,23 @@ struct Block {
 
 static std::mutex g_blk_mu;
 static std::map<int, std::vector<Block *>> g_blk_free;
-constexpr size_t kMaxCachedBlocks = 2;
+// released blocks kept per device: at most this many, and at most half of
+// the device's memory together
+constexpr size_t kMaxCachedBlocks = 8;
+
+static size_t device_total_bytes(int device)
+{
+    static std::mutex mu;
+    static std::map<int, size_t> total;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = total.find(device);
+    if (it != total.end()) return it->second;
+    cudaDeviceProp prop;
+    size_t t = cudaGetDeviceProperties(&prop, device) == cudaSuccess ? prop.totalGlobalMem : 0;
+    cudaGetLastError();
+    total[device] = t;
+    return t;
+}
 
 static bool trace_on()
 {
@@ -375,13 +393,18 @@ static Block *block_get(int device, size_t bytes)
 {
     {
         std::lock_guard<std::mutex> lk(g_blk_mu);
+        // the smallest cached block that holds the job and wastes at most a
+        // fifth of itself (tiles of a few neighbouring sizes share blocks)
         auto &v = g_blk_free[device];
-        for (size_t i = 0; i < v.size(); ++i) {
-            if (v[i]->bytes == bytes) {
-                Block *b = v[i];
-                v.erase(v.begin() + (long) i);
-                return b;
-            }
+        size_t best = v.size();
+        for (size_t i = 0; i < v.size(); ++i)
+            if (v[i]->bytes >= bytes && (double) v[i]->bytes <= 1.25 * (double) bytes &&
+                (best == v.size() || v[i]->bytes < v[best]->bytes))
+                best = i;
+        if (best < v.size()) {
+            Block *b = v[best];
+            v.erase(v.begin() + (long) best);
+            return b;
         }
     }
     Block *b = new Block();
@@ -415,7 +438,11 @@ static void block_put(Block *b)
         std::lock_guard<std::mutex> lk(g_blk_mu);
         auto &v = g_blk_free[b->device];
         v.push_back(b);
-        while (v.size() > kMaxCachedBlocks) {
+        const double cap = 0.5 * (double) device_total_bytes(b->device);
+        double held = 0;
+        for (auto *c : v) held += (double) c->bytes;
+        while (!v.empty() && (v.size() > kMaxCachedBlocks || held > cap)) {
+            held -= (double) v.front()->bytes;
             drop.push_back(v.front());
             v.erase(v.begin());
         }
@@ -1322,7 +1349,22 @@ static int one_call(const float *im, long long M, long long N, long long P, cons
     TRY(job_create(M, N, P, pM, pN, pP, s, &j));
     if (on_device && stream) j->stream = stream;
     int rc = job_setup(j, im, psf, on_device);
+    // a pageable result buffer is faulted in by a host thread while the
+    // device iterates, so that the result copy does not wait for it
+    std::thread prefault;
+    if (!on_device) {
+        cudaPointerAttributes pa;
+        const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        const size_t n = (size_t) (M * N * P);
+        if (!locked && rc == DWCU_SUCCESS)
+            prefault = std::thread([out, n]() {
+                const size_t chunk = (size_t) 1 << 22;
+                for (size_t i = 0; i < n; i += chunk) memset(out + i, 0, sizeof(float) * std::min(chunk, n - i));
+            });
+    }
     if (rc == DWCU_SUCCESS) rc = job_step(j, 1 << 30, nullptr);
+    if (prefault.joinable()) prefault.join();
     if (rc == DWCU_SUCCESS) rc = job_result(j, out, on_device, s);
     if (rc == DWCU_SUCCESS && s->bg_auto) s->bg = j->s.bg;
     dwcu_job_destroy(j);
@@ -1575,6 +1617,24 @@ int dwcu_job_result(dwcu_job *job, float *out, int32_t out_on_device, dwcu_opts 
 {
     if (!job || !out) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
     return job_result(job, out, out_on_device != 0, s_out);
+}
+
+int dwcu_release_cache(int32_t device)
+{
+    std::vector<Block *> drop;
+    {
+        std::lock_guard<std::mutex> lk(g_blk_mu);
+        for (auto &kv : g_blk_free) {
+            if (device >= 0 && kv.first != device) continue;
+            drop.insert(drop.end(), kv.second.begin(), kv.second.end());
+            kv.second.clear();
+        }
+    }
+    for (auto *b : drop) {
+        cudaSetDevice(b->device);
+        block_free(b);
+    }
+    return DWCU_SUCCESS;
 }
 
 void dwcu_job_destroy(dwcu_job *j)

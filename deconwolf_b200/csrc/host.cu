@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dwcu.h"
@@ -306,66 +307,131 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, cons
     TCU(cudaMemcpyAsync(d_tiles, ht.data(), sizeof(DevTile) * (size_t) nt, cudaMemcpyHostToDevice, st));
     TCU(cudaMemsetAsync(d_out, 0, sizeof(float) * nvox, st));
 
-    // per tile: PSF copy normalised and cropped against the tile (dw.c:2112-2130)
-    struct TileJob {
-        dwcu_job *job = nullptr;
+    // Pageable output pages are touched by a host thread while the tiles
+    // iterate, so that the final device-to-host copy does not fault them in
+    // (page-locked memory is resident already).
+    cudaPointerAttributes pa;
+    const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    std::thread prefault;
+    if (!locked)
+        prefault = std::thread([out, nvox]() {
+            const size_t chunk = (size_t) 1 << 22;
+            for (size_t i = 0; i < nvox; i += chunk) memset(out + i, 0, sizeof(float) * std::min(chunk, nvox - i));
+        });
+    struct Joiner {
+        std::thread &t;
+        ~Joiner() { if (t.joinable()) t.join(); }
+    } joiner{prefault};
+
+    // per tile: PSF copy normalised and cropped against the tile
+    // (dw.c:2112-2130); tiles of one size share the result
+    struct TilePsf {
+        int64_t xs[3];
         std::vector<float> psf;
-        int64_t d[3] = {0, 0, 0};
-        float *d_tile = nullptr;
-        float *d_psf = nullptr;
+        int64_t d[3];
+        float *dev = nullptr;
     };
-    std::vector<TileJob> tj((size_t) nt);
+    std::vector<TilePsf> psfs;
+    std::vector<int> psf_of((size_t) nt);
     for (int i = 0; i < nt; ++i) {
-        TileJob &T = tj[(size_t) i];
         const dwcu_tile &t = tiles[(size_t) i];
-        T.psf.assign(psf, psf + pM * pN * pP);
-        int64_t a = pM, b = pN, c = pP;
-        normalize_sum1(T.psf);
-        crop_by_image(T.psf, a, b, c, t.xsize[0], t.xsize[1], t.xsize[2], s->border_quality);
-        if (s->border_quality > 0 && xycropfactor > 0) crop_xy(T.psf, a, b, c, xycropfactor);
-        normalize_sum1(T.psf);
-        T.d[0] = a; T.d[1] = b; T.d[2] = c;
+        int k = 0;
+        while (k < (int) psfs.size() && !(psfs[(size_t) k].xs[0] == t.xsize[0] && psfs[(size_t) k].xs[1] == t.xsize[1] &&
+                                          psfs[(size_t) k].xs[2] == t.xsize[2]))
+            ++k;
+        if (k == (int) psfs.size()) {
+            TilePsf tp;
+            memcpy(tp.xs, t.xsize, sizeof tp.xs);
+            tp.psf.assign(psf, psf + pM * pN * pP);
+            int64_t a = pM, b = pN, c = pP;
+            normalize_sum1(tp.psf);
+            crop_by_image(tp.psf, a, b, c, t.xsize[0], t.xsize[1], t.xsize[2], s->border_quality);
+            if (s->border_quality > 0 && xycropfactor > 0) crop_xy(tp.psf, a, b, c, xycropfactor);
+            normalize_sum1(tp.psf);
+            tp.d[0] = a; tp.d[1] = b; tp.d[2] = c;
+            psfs.push_back(std::move(tp));
+        }
+        psf_of[(size_t) i] = k;
     }
-    // waves of tiles that fit the device-memory budget, each run as one batch
+    auto free_psfs = [&]() {
+        for (auto &tp : psfs)
+            if (tp.dev) cudaFree(tp.dev);
+    };
+    for (auto &tp : psfs) {
+        cudaError_t e = cudaMalloc(&tp.dev, sizeof(float) * tp.psf.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(tp.dev, tp.psf.data(), sizeof(float) * tp.psf.size(), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {
+            free_psfs();
+            cleanup();
+            return fail(e == cudaErrorMemoryAllocation ? DWCU_ERROR_OUT_OF_MEMORY : DWCU_ERROR_CUDA,
+                        "tile PSF upload failed: %s", cudaGetErrorString(e));
+        }
+    }
+    // waves of tiles that fit the device-memory budget, each run as one
+    // batch; a tile whose job fills the GPU on its own (>= 32 Mi padded
+    // voxels, which the batch runner would run one after another anyway)
+    // is a wave of its own, so that its job block is reused by the next
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     const double budget = hbm_budget > 0 ? hbm_budget : 0.85 * (double) free_b;
+    const double large = 32.0 * 1024 * 1024;
+    struct TileJob {
+        dwcu_job *job = nullptr;
+        float *d_tile = nullptr;
+    };
+    std::vector<TileJob> tj((size_t) nt);
+    std::vector<float *> bufs;  // tile buffers, reused by the waves
+    size_t buf_elems = 0;
+    for (const auto &t : tiles) buf_elems = std::max(buf_elems, (size_t) (t.xsize[0] * t.xsize[1] * t.xsize[2]));
     int next = 0;
     rc = DWCU_SUCCESS;
-    std::vector<float> trace_acc;
     while (next < nt && rc == DWCU_SUCCESS) {
         std::vector<int> wave;
         double used = 0;
         for (int i = next; i < nt; ++i) {
             const dwcu_tile &t = tiles[(size_t) i];
+            const TilePsf &tp = psfs[(size_t) psf_of[(size_t) i]];
             int64_t w3[3];
             int64_t need = 0;
-            rc = dwcu_plan_size(t.xsize[0], t.xsize[1], t.xsize[2], tj[(size_t) i].d[0], tj[(size_t) i].d[1],
-                                tj[(size_t) i].d[2], s->border_quality, s->method, w3, &need);
+            rc = dwcu_plan_size(t.xsize[0], t.xsize[1], t.xsize[2], tp.d[0], tp.d[1], tp.d[2], s->border_quality,
+                                s->method, w3, &need);
             if (rc) break;
+            const bool big = (double) w3[0] * (double) w3[1] * (double) w3[2] >= large;
             need += (int64_t) (sizeof(float) * (t.xsize[0] * t.xsize[1] * t.xsize[2]) * 2);
-            if (!wave.empty() && used + (double) need > budget) break;
+            if (!wave.empty() && (big || used + (double) need > budget)) break;
             used += (double) need;
             wave.push_back(i);
+            if (big) break;
         }
         if (rc) break;
-        std::vector<dwcu_job *> jobs;
-        for (int i : wave) {
-            TileJob &T = tj[(size_t) i];
-            const dwcu_tile &t = tiles[(size_t) i];
-            const size_t tv = (size_t) (t.xsize[0] * t.xsize[1] * t.xsize[2]);
-            if (cudaMalloc(&T.d_tile, sizeof(float) * tv) != cudaSuccess ||
-                cudaMalloc(&T.d_psf, sizeof(float) * T.psf.size()) != cudaSuccess) {
+        while (bufs.size() < wave.size()) {
+            float *b = nullptr;
+            if (cudaMalloc(&b, sizeof(float) * buf_elems) != cudaSuccess) {
                 rc = fail(DWCU_ERROR_OUT_OF_MEMORY, "tile buffers");
                 break;
             }
-            cudaMemcpyAsync(T.d_psf, T.psf.data(), sizeof(float) * T.psf.size(), cudaMemcpyHostToDevice, st);
+            bufs.push_back(b);
+        }
+        if (rc) break;
+        std::vector<dwcu_job *> jobs;
+        for (size_t w = 0; w < wave.size(); ++w) {
+            const int i = wave[w];
+            TileJob &T = tj[(size_t) i];
+            const dwcu_tile &t = tiles[(size_t) i];
+            const TilePsf &tp = psfs[(size_t) psf_of[(size_t) i]];
+            const size_t tv = (size_t) (t.xsize[0] * t.xsize[1] * t.xsize[2]);
+            T.d_tile = bufs[w];
             const int blocks = (int) std::min<size_t>(4096, (tv + 255) / 256);
             k_tile_extract<<<blocks, 256, 0, st>>>(d_im, M, N, ht[(size_t) i], offset, T.d_tile);
             dwcu::record_launch();
-            cudaStreamSynchronize(st);
-            rc = dwcu_job_create(t.xsize[0], t.xsize[1], t.xsize[2], T.d[0], T.d[1], T.d[2], s, &T.job);
-            if (rc == DWCU_SUCCESS) rc = dwcu_job_setup(T.job, T.d_tile, T.d_psf, 1);
+            if (cudaStreamSynchronize(st) != cudaSuccess) {
+                rc = fail(DWCU_ERROR_CUDA, "tile extraction failed");
+                break;
+            }
+            rc = dwcu_job_create(t.xsize[0], t.xsize[1], t.xsize[2], tp.d[0], tp.d[1], tp.d[2], s, &T.job);
+            if (rc == DWCU_SUCCESS) rc = dwcu_job_setup(T.job, T.d_tile, tp.dev, 1);
             if (rc) break;
             jobs.push_back(T.job);
         }
@@ -385,27 +451,25 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, cons
                     const int blocks = (int) std::min<size_t>(4096, (tv + 255) / 256);
                     k_tile_blend<<<blocks, 256, 0, st>>>(T.d_tile, M, N, d_tiles, nt, i, offset, d_out);
                     dwcu::record_launch();
-                    cudaStreamSynchronize(st);
+                    if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "tile blend failed");
                 }
             }
             if (T.job) dwcu_job_destroy(T.job);
             T.job = nullptr;
-            if (T.d_tile) cudaFree(T.d_tile);
-            if (T.d_psf) cudaFree(T.d_psf);
-            T.d_tile = T.d_psf = nullptr;
+            T.d_tile = nullptr;
         }
         next = wave.empty() ? nt : wave.back() + 1;
     }
+    if (prefault.joinable()) prefault.join();
     if (rc == DWCU_SUCCESS) {
         cudaError_t e = cudaMemcpyAsync(out, d_out, sizeof(float) * nvox, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "result copy failed: %s", cudaGetErrorString(e));
     }
-    for (auto &T : tj) {
+    for (auto *b : bufs) cudaFree(b);
+    free_psfs();
+    for (auto &T : tj)
         if (T.job) dwcu_job_destroy(T.job);
-        if (T.d_tile) cudaFree(T.d_tile);
-        if (T.d_psf) cudaFree(T.d_psf);
-    }
     cleanup();
 #undef TCU
     return rc;

@@ -87,6 +87,10 @@ CONFIGS = {
                             seed=5),
     "shb-256x256x60": dict(shape=(60, 256, 256), psf_shape=(119, 181, 181), lam=670.0, K=600, B=9, bg=100.0,
                            seed=6),
+    # one interior tile of the 4096^2 x 60 image at tile size 1024 and
+    # overlap 50 (1124^2 x 60, job 1344^2 x 180)
+    "shb-1124x1124x60": dict(shape=(60, 1124, 1124), psf_shape=(119, 181, 181), lam=670.0, K=12000, B=180,
+                             bg=100.0, seed=7),
 }
 
 

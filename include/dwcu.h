@@ -144,8 +144,14 @@ int dwcu_job_done(const dwcu_job *job);
 /* Wait for the job's queued work; copy the result (host or device pointer)
  * and the error trace.  Fills s-like outputs into *s_out when non-NULL. */
 int dwcu_job_result(dwcu_job *job, float *out, int32_t out_on_device, dwcu_opts *s_out);
-/* Release all device memory of the job. */
+/* Release the job.  Its device block is kept by the library for the next
+ * job of a similar size (at most eight blocks and half of the device's
+ * memory per device); dwcu_release_cache frees those. */
 void dwcu_job_destroy(dwcu_job *job);
+/* Free the device blocks the library keeps for reuse on `device` (all
+ * devices when negative).  No counterpart in the reference, which allocates
+ * per call. */
+int dwcu_release_cache(int32_t device);
 /* Use a caller stream (cudaStream_t) for this job's work. */
 int dwcu_job_set_stream(dwcu_job *job, void *stream);
 /* Device bytes held by the job. */

@@ -102,3 +102,8 @@ def test_no_gpu_server_and_tiles_fail():
     with pytest.raises(dw.DwcuError) as e:
         dw.deconvolve_tiled(im, psf, 20, 4, n_iter=2)
     assert e.value.code == 4
+
+
+def test_release_cache_without_blocks():
+    dw.release_cache()
+    dw.release_cache(0)

@@ -258,3 +258,16 @@ def test_fft_r2c_matches_oracle(shape):
     y2 = d_y.cpu().numpy() / np.float32(P * N * M)
     assert np.max(np.abs(y2 - xx) / xx) < 1e-5
     assert np.max(np.abs(y - x)) < 1e-5
+
+
+def test_block_reuse_and_release():
+    """Jobs of neighbouring sizes reuse cached device blocks; results do not
+    depend on which block a job got, and freeing the cache changes nothing."""
+    im, psf = case_inputs(seed=8, shape=(12, 40, 44), psf_shape=(5, 7, 9))
+    a = dw.run_method(im, psf, method="shb", n_iter=6)
+    b = dw.run_method(im[:, :38, :42], psf, method="shb", n_iter=6)  # smaller job, may take a's block
+    c = dw.run_method(im, psf, method="shb", n_iter=6)
+    dw.release_cache()
+    d = dw.run_method(im[:, :38, :42], psf, method="shb", n_iter=6)
+    np.testing.assert_array_equal(a.out, c.out)
+    np.testing.assert_array_equal(b.out, d.out)
