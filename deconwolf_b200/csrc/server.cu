@@ -23,6 +23,7 @@
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
+#include <cstring>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -68,6 +69,13 @@ struct Request {
     cudaStream_t stream = nullptr;
     std::deque<cudaEvent_t> inflight;  // one event per chunk not yet known complete
     int remaining = 0;
+    // faults a pageable result buffer in while the request waits and runs
+    std::thread prefault;
+    void join_prefault()
+    {
+        if (prefault.joinable()) prefault.join();
+    }
+    ~Request() { join_prefault(); }
 };
 
 }  // namespace
@@ -110,6 +118,7 @@ struct dwcu_server {
     void finish(Request *r, int status)
     {
         // called by the worker without the lock held; the job's stream is idle
+        r->join_prefault();
         if (r->job) {
             dwcu_job_destroy(r->job);
             r->job = nullptr;
@@ -181,6 +190,7 @@ struct dwcu_server {
                 while (!queue.empty() && (int) active.size() + (int) to_start.size() < max_active) {
                     Request *r = queue.front();
                     if (r->cancel) {
+                        r->join_prefault();  // the caller may free the buffer once it sees the status
                         queue.pop_front();
                         r->status = DWCU_ERROR_CANCELLED;
                         ++cancelled;
@@ -229,6 +239,7 @@ struct dwcu_server {
                     r->result = r->opts;
                     r->result.error_trace = r->opts.error_trace;
                     r->result.trace_capacity = r->opts.trace_capacity;
+                    r->join_prefault();
                     const int rc = dwcu_job_result(r->job, r->out, 0, &r->result);
                     finish(r, rc);
                     progressed = true;
@@ -304,6 +315,23 @@ int dwcu_server_submit(dwcu_server *sv, const float *im, int64_t M, int64_t N, i
     r->opts = *s;
     r->need = need;
     r->t_submit = clk::now();
+    {
+        // (asked on the server's device; the caller's current device is restored)
+        int cur = 0;
+        const bool had = cudaGetDevice(&cur) == cudaSuccess;
+        cudaSetDevice(sv->device);
+        cudaPointerAttributes pa;
+        const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (had) cudaSetDevice(cur);
+        if (!locked) {
+            const size_t n = (size_t) (M * N * P);
+            r->prefault = std::thread([out, n]() {
+                const size_t chunk = (size_t) 1 << 22;
+                for (size_t i = 0; i < n; i += chunk) memset(out + i, 0, sizeof(float) * std::min(chunk, n - i));
+            });
+        }
+    }
     std::lock_guard<std::mutex> lk(sv->mu);
     if (sv->stop) {
         delete r;
