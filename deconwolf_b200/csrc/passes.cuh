@@ -90,9 +90,22 @@ __device__ __forceinline__ void butterfly(float2 (&v)[Q][R], const float2 (&w)[R
 // exchange tiles may be reused by the caller only after another barrier.
 // PREF: load each stage's twiddles before the barrier that precedes the
 // stage (hides their latency; costs registers across the barrier).
+// PP (ping-pong): stage 2 writes a second exchange tile, smem2, so that no
+// barrier is needed between its reads and its writes; stage 3 reads smem2.
+template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2>
+__device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
+                                              const float2 *__restrict__ tw, SM smem, SM2 smem2);
+
 template <class RD, int DIR, int Q, bool PREF = false, class SM>
 __device__ __forceinline__ void line_fft(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
                                          const float2 *__restrict__ tw, SM smem)
+{
+    line_fft_impl<RD, DIR, Q, PREF, false>(v, o, t, tw, smem, smem);
+}
+
+template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2>
+__device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
+                                              const float2 *__restrict__ tw, SM smem, SM2 smem2)
 {
     constexpr int N = RD::N, RA = RD::RA, RB = RD::RB, RC = RD::RC;
     constexpr int M2 = N / RB;  // stage-2 butterflies; read stride, a multiple of RA
@@ -119,7 +132,7 @@ __device__ __forceinline__ void line_fft(float2 (&v)[Q][RD::RA], float2 (&o)[Q][
 #pragma unroll
                 for (int r = 0; r < RB; ++r) u[q][r] = *smem(q, b2 + r * (M2 + M2 / RA));
         }
-        __syncthreads();
+        if constexpr (!PP) __syncthreads();
         if (t < M2) {
             if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
             butterfly<RA, RB, DIR, Q>(u, w2);
@@ -128,7 +141,7 @@ __device__ __forceinline__ void line_fft(float2 (&v)[Q][RD::RA], float2 (&o)[Q][
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
-                for (int r = 0; r < RB; ++r) *smem(q, b3 + r * (RA + 1)) = u[q][r];
+                for (int r = 0; r < RB; ++r) *smem2(q, b3 + r * (RA + 1)) = u[q][r];
         }
         float2 w3[RC];
         if (PREF && t < M3) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
@@ -138,7 +151,7 @@ __device__ __forceinline__ void line_fft(float2 (&v)[Q][RD::RA], float2 (&o)[Q][
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
-                for (int r = 0; r < RC; ++r) o[q][r] = *smem(q, b4 + r * (M3 + M3 / RA));
+                for (int r = 0; r < RC; ++r) o[q][r] = *smem2(q, b4 + r * (M3 + M3 / RA));
             if (!PREF) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
             butterfly<RA * RB, RC, DIR, Q>(o, w3);
         }
@@ -300,7 +313,11 @@ struct YCfg {
     static constexpr int TX = KB / Q;            // threads across the 4 lines
     static constexpr int THREADS = TX * RD::TPL;
     static constexpr int BUF_F2 = RD::PADN * KB;
-    static constexpr size_t SMEM_BYTES = 2 * sizeof(float2) * (size_t) BUF_F2 + 64;
+    // two tile buffers (the next tile's copy lands in one while the other is
+    // transformed) and, where it fits, a third exchange tile so that the
+    // transform's stages need fewer barriers (line_fft_impl, PP)
+    static constexpr bool PP = 3 * sizeof(float2) * (size_t) BUF_F2 + 64 <= 227 * 1024;
+    static constexpr size_t SMEM_BYTES = (PP ? 3 : 2) * sizeof(float2) * (size_t) BUF_F2 + 64;
     static constexpr uint32_t TILE_BYTES = (uint32_t) (RD::N * KB * sizeof(float2));
 };
 
@@ -354,10 +371,18 @@ k_ypass(YArgs a)
 #pragma unroll
                 for (int q = 0; q < Q; ++q) v[q][r] = buf[(t + r * (N / RD::RA)) * KB + l0 + q];
         }
-        __syncthreads();  // natural-order reads done; the buffer becomes the exchange tile
         auto smem = [&](int q, int i) { return buf + (size_t) i * KB + l0 + q; };
         float2 o[Q][RD::RL];
-        line_fft<RD, DIR, Q>(v, o, t, a.tw, smem);
+        if constexpr (C::PP) {
+            // stage 1 writes the third tile (no barrier after the natural-order
+            // reads), stage 2 writes the tile buffer back
+            float2 *ex = bufs + (size_t) 2 * C::BUF_F2;
+            auto smemx = [&](int q, int i) { return ex + (size_t) i * KB + l0 + q; };
+            line_fft_impl<RD, DIR, Q, false, true>(v, o, t, a.tw, smemx, smem);
+        } else {
+            __syncthreads();  // natural-order reads done; the buffer becomes the exchange tile
+            line_fft<RD, DIR, Q>(v, o, t, a.tw, smem);
+        }
         constexpr int SL = N / RD::RL;
         if (t < SL) {
             float2 *dst = a.data + (size_t) tile * N * KB + l0;
