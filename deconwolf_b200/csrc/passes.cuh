@@ -479,7 +479,12 @@ struct XCfg {
     // complex area and three real slots: x (or the image rows g, which no op
     // reads together with x), xp, W
     static constexpr size_t REAL_OFF = 64 + sizeof(float2) * (size_t) AREA_F2;
-    static constexpr size_t RED_OFF = REAL_OFF + x_slots(FAM) * sizeof(float) * (size_t) REAL_F;
+    // the real slots are also the forward transform's second exchange tile
+    // (read by the pointwise op before it), so they hold R padded rows
+    static constexpr size_t SLOT_BYTES = x_slots(FAM) * sizeof(float) * (size_t) REAL_F;
+    static constexpr size_t XCH2_BYTES = FAM == 3 ? 0 : sizeof(float2) * (size_t) (R * ROW_F2);
+    static constexpr size_t REAL_BYTES = SLOT_BYTES > XCH2_BYTES ? SLOT_BYTES : XCH2_BYTES;
+    static constexpr size_t RED_OFF = REAL_OFF + (REAL_BYTES + 7) / 8 * 8;
     static constexpr size_t SMEM_BYTES = RED_OFF + sizeof(double) * THREADS;
     // resident CTAs per SM to aim for (registers are capped to fit them)
     // (one-row update tiles, family 2: five CTAs, which caps registers at 72)
@@ -916,9 +921,13 @@ k_xpass(XArgs a)
         __syncthreads();
     }
     float2 qo[Q][RV::RL];
-    line_fft<RV, -1, Q, PREF_TW>(w, qo, t, a.twL, smem);
+    // stage 2 writes the real slots (every pointwise read of them precedes
+    // the barrier after stage 1), so stage 3 leaves the exchange tiles free
+    float2 *xb2 = reinterpret_cast<float2 *>(RB);
+    auto smem2 = [&](int q, int i) { return xb2 + (size_t) (ry * Q + q) * C::ROW_F2 + i; };
+    line_fft_impl<RV, -1, Q, PREF_TW, true>(w, qo, t, a.twL, smem, smem2);
     constexpr int SQ = L / RV::RL;
-    __syncthreads();
+    if constexpr (!RV::THREE) __syncthreads();
     if (t < SQ) {
 #pragma unroll
         for (int q = 0; q < Q; ++q)
