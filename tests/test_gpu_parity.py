@@ -271,3 +271,28 @@ def test_block_reuse_and_release():
     d = dw.run_method(im[:, :38, :42], psf, method="shb", n_iter=6)
     np.testing.assert_array_equal(a.out, c.out)
     np.testing.assert_array_equal(b.out, d.out)
+
+
+
+
+EVEN_CASES = [
+    # (image, PSF, border_quality, method): PSFs even about their centre, as
+    # the Born-Wolf and Gaussian models are
+    ((12, 40, 44), (7, 9, 11), 2, "shb"),
+    ((12, 40, 44), (7, 9, 11), 2, "rl"),
+    ((9, 22, 20), (5, 7, 9), 1, "shb"),     # periodic margins in x and y
+    ((20, 33, 44), (21, 15, 13), 0, "shb"),
+    ((1, 64, 60), (1, 9, 9), 2, "shb"),     # a single plane
+]
+
+
+@pytest.mark.parametrize("shape,psf_shape,bq,method", EVEN_CASES)
+def test_even_psf(shape, psf_shape, bq, method):
+    """Exactly even PSFs (unjittered Gaussians): results as the reference's."""
+    psf = gauss_psf(psf_shape, (1.3, 1.6, 1.9))
+    assert np.array_equal(psf, psf[::-1, ::-1, ::-1])
+    im = poisson_image(shape, psf, seed=11, bg=40.0, npts=12)
+    g = dw.run_method(im, psf, border_quality=bq, method=method, n_iter=8)
+    r = po.deconvolve(im, psf, border_quality=bq, method=method, n_iter=8, impl=checker())
+    assert rel_l2(g.out, r.out) < OUT_TOL
+    assert trace_err(g.trace, r.trace) < TRACE_TOL
