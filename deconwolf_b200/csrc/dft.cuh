@@ -67,8 +67,29 @@ DW_HD void static_for(F &&f)
     static_for_impl(f, std::make_integer_sequence<int, N>{});
 }
 
-DW_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-DW_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// complex sums as one paired single-precision add on sm_100 (FADD2: both
+// lanes rounded to nearest, as two scalar adds).  A translation unit may
+// define DW_PAIRED_ADDS 0 first to keep scalar adds (device code is compiled
+// per translation unit).
+#ifndef DW_PAIRED_ADDS
+#define DW_PAIRED_ADDS 1
+#endif
+DW_HD float2 cadd(float2 a, float2 b)
+{
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && DW_PAIRED_ADDS
+    return __fadd2_rn(a, b);
+#else
+    return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+DW_HD float2 csub(float2 a, float2 b)
+{
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && DW_PAIRED_ADDS
+    return __fadd2_rn(a, make_float2(-b.x, -b.y));
+#else
+    return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
 DW_HD float2 cmul(float2 a, float2 b)
 {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);

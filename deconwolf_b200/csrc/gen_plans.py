@@ -202,7 +202,11 @@ def main():
     for kind, ns in (("lines", lines_ns), ("x", x_ns), ("y", y_ns)):
         for p in range(parts):
             chunk = ns[p::parts]
-            lines = ["// generated by gen_plans.py -- do not edit", "#include \"launch.cuh\"", "namespace dwcu {"]
+            lines = ["// generated by gen_plans.py -- do not edit"]
+            if kind == "y":
+                # the y pass runs faster with scalar complex adds (dft.cuh)
+                lines.append("#define DW_PAIRED_ADDS 0")
+            lines += ["#include \"launch.cuh\"", "namespace dwcu {"]
             for n in chunk:
                 s = best_split(n)
                 if kind == "lines":

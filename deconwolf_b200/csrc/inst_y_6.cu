@@ -1,4 +1,5 @@
 // generated by gen_plans.py -- do not edit
+#define DW_PAIRED_ADDS 0
 #include "launch.cuh"
 namespace dwcu {
 void launch_y_8(const YArgs &a, cudaStream_t st) { launch_y_t<Rad<4, 2, 1>>(a, st); }
