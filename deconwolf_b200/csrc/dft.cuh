@@ -202,10 +202,15 @@ struct DftOddPrime {
                 constexpr int j = decltype(jj)::value + 1;
                 constexpr float c = (float) cx::cospi_frac(2 * j * q, N);
                 constexpr float s = (float) cx::sinpi_frac(2 * j * q, N);
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && DW_PAIRED_ADDS
+                e = __ffma2_rn(make_float2(c, c), A[j], e);
+                f = __ffma2_rn(make_float2(s, s), B[j], f);
+#else
                 e.x = fmaf(c, A[j].x, e.x);
                 e.y = fmaf(c, A[j].y, e.y);
                 f.x = fmaf(s, B[j].x, f.x);
                 f.y = fmaf(s, B[j].y, f.y);
+#endif
             });
             // X_q = e + DIR*i*f ; X_{N-q} = e - DIR*i*f
             float2 r = mul_i<DIR>(f);
