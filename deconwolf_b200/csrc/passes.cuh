@@ -63,6 +63,21 @@ __device__ __forceinline__ void stage_twiddles(float2 (&w)[R], int j, const floa
 #pragma unroll
     for (int r = 2; r < R; ++r) w[r] = (r % 2 == 0) ? cmul(w[r / 2], w[r / 2]) : cmul(w[r - 1], w[1]);
 }
+// the table value stage_twiddles loads (for callers that keep it in a register)
+template <int N, int NS, int R>
+__device__ __forceinline__ float2 stage_twiddle_base(int j, const float2 *__restrict__ tw)
+{
+    constexpr int step = N / (NS * R);
+    return __ldg(&tw[(j % NS) * step]);
+}
+// stage_twiddles from that value
+template <int R>
+__device__ __forceinline__ void stage_twiddles_from(float2 (&w)[R], float2 b)
+{
+    if constexpr (R > 1) w[1] = b;
+#pragma unroll
+    for (int r = 2; r < R; ++r) w[r] = (r % 2 == 0) ? cmul(w[r / 2], w[r / 2]) : cmul(w[r - 1], w[1]);
+}
 
 // one Stockham butterfly on Q rows that share the butterfly index:
 // v[q][r] = x_q[j + r*N/R] on entry, multiplied by the stage twiddles w[r]
@@ -92,9 +107,12 @@ __device__ __forceinline__ void butterfly(float2 (&v)[Q][R], const float2 (&w)[R
 // stage (hides their latency; costs registers across the barrier).
 // PP (ping-pong): stage 2 writes a second exchange tile, smem2, so that no
 // barrier is needed between its reads and its writes; stage 3 reads smem2.
-template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2>
+// HOIST: the stage twiddles come from tb2 / tb3 (stage_twiddle_base of
+// stages 2 and 3 for this thread, kept by the caller) instead of the table
+template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2, bool HOIST = false>
 __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
-                                              const float2 *__restrict__ tw, SM smem, SM2 smem2);
+                                              const float2 *__restrict__ tw, SM smem, SM2 smem2,
+                                              float2 tb2 = float2{}, float2 tb3 = float2{});
 
 template <class RD, int DIR, int Q, bool PREF = false, class SM>
 __device__ __forceinline__ void line_fft(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
@@ -103,9 +121,10 @@ __device__ __forceinline__ void line_fft(float2 (&v)[Q][RD::RA], float2 (&o)[Q][
     line_fft_impl<RD, DIR, Q, PREF, false>(v, o, t, tw, smem, smem);
 }
 
-template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2>
+template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2, bool HOIST>
 __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
-                                              const float2 *__restrict__ tw, SM smem, SM2 smem2)
+                                              const float2 *__restrict__ tw, SM smem, SM2 smem2, float2 tb2,
+                                              float2 tb3)
 {
     constexpr int N = RD::N, RA = RD::RA, RB = RD::RB, RC = RD::RC;
     constexpr int M2 = N / RB;  // stage-2 butterflies; read stride, a multiple of RA
@@ -134,7 +153,8 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
         }
         if constexpr (!PP) __syncthreads();
         if (t < M2) {
-            if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
+            if constexpr (HOIST) stage_twiddles_from<RB>(w2, tb2);
+            else if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
             butterfly<RA, RB, DIR, Q>(u, w2);
             const int base = (t / RA) * RA * RB + t % RA;  // writes base + r*RA
             const int b3 = base + base / RA;
@@ -152,7 +172,8 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
             for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int r = 0; r < RC; ++r) o[q][r] = *smem2(q, b4 + r * (M3 + M3 / RA));
-            if (!PREF) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
+            if constexpr (HOIST) stage_twiddles_from<RC>(w3, tb3);
+            else if (!PREF) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
             butterfly<RA * RB, RC, DIR, Q>(o, w3);
         }
     } else {
@@ -162,7 +183,8 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
             for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int r = 0; r < RB; ++r) o[q][r] = *smem(q, b2 + r * (M2 + M2 / RA));
-            if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
+            if constexpr (HOIST) stage_twiddles_from<RB>(w2, tb2);
+            else if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
             butterfly<RA, RB, DIR, Q>(o, w2);
         }
     }
@@ -343,6 +365,11 @@ k_ypass(YArgs a)
         fence_mbar_init();
     }
     __syncthreads();
+    // this thread's stage twiddle values are the same for every tile
+    const float2 tb2 = stage_twiddle_base<N, RD::RA, RD::RB>(t < N / RD::RB ? t : 0, a.tw);
+    const float2 tb3 = RD::THREE ? stage_twiddle_base<N, RD::RA * RD::RB, (RD::THREE ? RD::RC : 1)>(
+                                       t < N / (RD::THREE ? RD::RC : 1) ? t : 0, a.tw)
+                                 : make_float2(1.f, 0.f);
     int tile = blockIdx.x;
     if (tid == 0 && tile < a.ntiles) {
         mbar_arrive_expect_tx(&bars[0], C::TILE_BYTES);
@@ -378,7 +405,8 @@ k_ypass(YArgs a)
             // reads), stage 2 writes the tile buffer back
             float2 *ex = bufs + (size_t) 2 * C::BUF_F2;
             auto smemx = [&](int q, int i) { return ex + (size_t) i * KB + l0 + q; };
-            line_fft_impl<RD, DIR, Q, false, true>(v, o, t, a.tw, smemx, smem);
+            line_fft_impl<RD, DIR, Q, false, true, decltype(smemx), decltype(smem), true>(v, o, t, a.tw, smemx,
+                                                                                          smem, tb2, tb3);
         } else {
             __syncthreads();  // natural-order reads done; the buffer becomes the exchange tile
             line_fft<RD, DIR, Q>(v, o, t, a.tw, smem);
