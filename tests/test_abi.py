@@ -107,3 +107,16 @@ def test_no_gpu_server_and_tiles_fail():
 def test_release_cache_without_blocks():
     dw.release_cache()
     dw.release_cache(0)
+
+
+def test_output_buffer_validation():
+    """A caller's result buffer must be a C-contiguous float32 array of the
+    image's shape; anything else is rejected before the library is called."""
+    im = np.ones((4, 8, 8), np.float32)
+    psf = np.ones((3, 3, 3), np.float32) / 27
+    for bad in (np.empty((4, 8, 9), np.float32), np.empty((4, 8, 8), np.float64),
+                np.empty((4, 8, 16), np.float32)[:, :, ::2]):
+        with pytest.raises(ValueError):
+            dw.run_method(im, psf, out=bad, n_iter=2)
+        with pytest.raises(ValueError):
+            dw.deconvolve_tiled(im, psf, 4, 1, out=bad, n_iter=2)
