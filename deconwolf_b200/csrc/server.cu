@@ -324,8 +324,10 @@ int dwcu_server_submit(dwcu_server *sv, const float *im, int64_t M, int64_t N, i
         const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
         cudaGetLastError();
         if (had) cudaSetDevice(cur);
-        if (!locked) {
-            const size_t n = (size_t) (M * N * P);
+        // (not when the result overwrites the image, which is uploaded later)
+        const size_t n = (size_t) (M * N * P);
+        const bool overlap = out < im + n && im < out + n;
+        if (!locked && !overlap) {
             r->prefault = std::thread([out, n]() {
                 const size_t chunk = (size_t) 1 << 22;
                 for (size_t i = 0; i < n; i += chunk) memset(out + i, 0, sizeof(float) * std::min(chunk, n - i));
