@@ -90,13 +90,24 @@ DW_HD float2 csub(float2 a, float2 b)
     return make_float2(a.x - b.x, a.y - b.y);
 #endif
 }
+// complex products: with paired instructions, one FMUL2 and one FFMA2
 DW_HD float2 cmul(float2 a, float2 b)
 {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && DW_PAIRED_ADDS
+    const float2 t = __fmul2_rn(a, make_float2(b.x, b.x));
+    return __ffma2_rn(make_float2(-a.y, a.x), make_float2(b.y, b.y), t);
+#else
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+#endif
 }
 DW_HD float2 cmulc(float2 a, float2 b)  // a * conj(b)
 {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && DW_PAIRED_ADDS
+    const float2 t = __fmul2_rn(a, make_float2(b.x, b.x));
+    return __ffma2_rn(make_float2(a.y, -a.x), make_float2(b.y, b.y), t);
+#else
     return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+#endif
 }
 // multiply by DIR*i
 template <int DIR>
