@@ -1630,10 +1630,13 @@ int dwcu_release_cache(int32_t device)
             kv.second.clear();
         }
     }
+    int cur = 0;
+    const bool had = cudaGetDevice(&cur) == cudaSuccess;
     for (auto *b : drop) {
         cudaSetDevice(b->device);
         block_free(b);
     }
+    if (had && !drop.empty()) cudaSetDevice(cur);  // the caller's current device as it was
     return DWCU_SUCCESS;
 }
 
