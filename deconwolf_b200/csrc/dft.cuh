@@ -136,11 +136,19 @@ DW_HD float2 twiddle(float2 v)
         constexpr float s = (float) (DIR * cx::sinpi_frac(2 * k, N));
         constexpr float sc = c > 0 ? h : -h;
         constexpr float ss = s > 0 ? h : -h;
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && DW_PAIRED_ADDS
+        return __ffma2_rn(make_float2(-v.y, v.x), make_float2(ss, ss), __fmul2_rn(v, make_float2(sc, sc)));
+#else
         return make_float2(sc * v.x - ss * v.y, ss * v.x + sc * v.y);
+#endif
     } else {
         constexpr float c = (float) cx::cospi_frac(2 * k, N);
         constexpr float s = (float) (DIR * cx::sinpi_frac(2 * k, N));
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && DW_PAIRED_ADDS
+        return __ffma2_rn(make_float2(-v.y, v.x), make_float2(s, s), __fmul2_rn(v, make_float2(c, c)));
+#else
         return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
+#endif
     }
 }
 
