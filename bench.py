@@ -41,7 +41,7 @@ WORKLOAD = "shb-2048x2048x60"
 SMALL = "shb-256x256x40"
 PROFILE_CASE = "shb-1024x1024x20"  # hardware-counter captures (profiles/)
 ITERS = 50
-# generated inputs are cached between runs of one machine (kept out of git and gpurun snapshots)
+# generated inputs are cached between runs on one machine (kept out of git)
 CACHE = os.environ.get("DWCU_INPUT_CACHE", os.path.join(ROOT, "_cache"))
 
 
