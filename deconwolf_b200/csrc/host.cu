@@ -99,20 +99,22 @@ static void crop_by_image(std::vector<float> &psf, int64_t &pM, int64_t &pN, int
 // xycropfactor times the largest one; float sums as in the reference
 static void crop_xy(std::vector<float> &psf, int64_t &pM, int64_t &pN, int64_t pP, float xycropfactor)
 {
+    // every x plane's sum in the reference's order (y outer, z inner), all
+    // planes at once so that the reads run along x
+    std::vector<float> plane((size_t) pM, 0.f);
+    for (int64_t yy = 0; yy < pN; ++yy)
+        for (int64_t zz = 0; zz < pP; ++zz) {
+            const float *row = psf.data() + (size_t) (yy * pM + zz * pM * pN);
+            for (int64_t xx = 0; xx < pM; ++xx) plane[(size_t) xx] += row[xx];
+        }
     float maxsum = 0;
-    for (int64_t xx = 0; xx < pM; ++xx) {
-        float sum = 0;
-        for (int64_t yy = 0; yy < pN; ++yy)
-            for (int64_t zz = 0; zz < pP; ++zz) sum += psf[(size_t) (xx + yy * pM + zz * pM * pN)];
-        if (sum > maxsum) maxsum = sum;
-    }
+    for (int64_t xx = 0; xx < pM; ++xx)
+        if (plane[(size_t) xx] > maxsum) maxsum = plane[(size_t) xx];
     int64_t first = -1;
     float sum = 0;
     while (sum < xycropfactor * maxsum && first + 1 < pM) {
         first++;
-        sum = 0;
-        for (int64_t yy = 0; yy < pN; ++yy)
-            for (int64_t zz = 0; zz < pP; ++zz) sum += psf[(size_t) (first + yy * pM + zz * pM * pN)];
+        sum = plane[(size_t) first];
     }
     if (first < 1) return;
     if (pM - 2 * first < 1 || pN - 2 * first < 1) return;
