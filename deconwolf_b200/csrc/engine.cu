@@ -1357,7 +1357,8 @@ static int one_call(const float *im, long long M, long long N, long long P, cons
         const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
         cudaGetLastError();
         const size_t n = (size_t) (M * N * P);
-        if (!locked && rc == DWCU_SUCCESS)
+        const bool overlap = out < im + n && im < out + n;  // an in-place call
+        if (!locked && !overlap && rc == DWCU_SUCCESS)
             prefault = std::thread([out, n]() {
                 const size_t chunk = (size_t) 1 << 22;
                 for (size_t i = 0; i < n; i += chunk) memset(out + i, 0, sizeof(float) * std::min(chunk, n - i));

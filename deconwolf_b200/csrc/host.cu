@@ -312,11 +312,13 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, cons
     // Pageable output pages are touched by a host thread while the tiles
     // iterate, so that the final device-to-host copy does not fault them in
     // (page-locked memory is resident already).
+    // (not when the result buffer is the image itself)
     cudaPointerAttributes pa;
     const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
     cudaGetLastError();
+    const bool overlap = out < im + nvox && im < out + nvox;
     std::thread prefault;
-    if (!locked)
+    if (!locked && !overlap)
         prefault = std::thread([out, nvox]() {
             const size_t chunk = (size_t) 1 << 22;
             for (size_t i = 0; i < nvox; i += chunk) memset(out + i, 0, sizeof(float) * std::min(chunk, nvox - i));
