@@ -316,9 +316,9 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, cons
     cudaPointerAttributes pa;
     const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    const bool overlap = out < im + nvox && im < out + nvox;
+    const bool aliased = out < im + nvox && im < out + nvox;
     std::thread prefault;
-    if (!locked && !overlap)
+    if (!locked && !aliased)
         prefault = std::thread([out, nvox]() {
             const size_t chunk = (size_t) 1 << 22;
             for (size_t i = 0; i < nvox; i += chunk) memset(out + i, 0, sizeof(float) * std::min(chunk, nvox - i));
