@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -1357,7 +1358,8 @@ static int one_call(const float *im, long long M, long long N, long long P, cons
         const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
         cudaGetLastError();
         const size_t n = (size_t) (M * N * P);
-        const bool overlap = out < im + n && im < out + n;  // an in-place call
+        const uintptr_t o0 = (uintptr_t) out, i0 = (uintptr_t) im, nb = sizeof(float) * n;
+        const bool overlap = o0 < i0 + nb && i0 < o0 + nb;  // an in-place call
         if (!locked && !overlap && rc == DWCU_SUCCESS)
             prefault = std::thread([out, n]() {
                 const size_t chunk = (size_t) 1 << 22;

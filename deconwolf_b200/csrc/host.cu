@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -316,7 +317,8 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, cons
     cudaPointerAttributes pa;
     const bool locked = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    const bool aliased = out < im + nvox && im < out + nvox;
+    const uintptr_t o0 = (uintptr_t) out, i0 = (uintptr_t) im, nb = sizeof(float) * nvox;
+    const bool aliased = o0 < i0 + nb && i0 < o0 + nb;
     std::thread prefault;
     if (!locked && !aliased)
         prefault = std::thread([out, nvox]() {

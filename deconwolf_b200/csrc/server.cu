@@ -23,6 +23,7 @@
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -326,7 +327,8 @@ int dwcu_server_submit(dwcu_server *sv, const float *im, int64_t M, int64_t N, i
         if (had) cudaSetDevice(cur);
         // (not when the result overwrites the image, which is uploaded later)
         const size_t n = (size_t) (M * N * P);
-        const bool overlap = out < im + n && im < out + n;
+        const uintptr_t o0 = (uintptr_t) out, i0 = (uintptr_t) im, nb = sizeof(float) * n;
+        const bool overlap = o0 < i0 + nb && i0 < o0 + nb;
         if (!locked && !overlap) {
             r->prefault = std::thread([out, n]() {
                 const size_t chunk = (size_t) 1 << 22;
