@@ -4,13 +4,14 @@ Writes, next to this file:
   plans_gen.h         the table of supported line lengths with their radix
                       lists and launch shapes (lines: T lines per CTA;
                       x pass: R rows per CTA)
-  inst_lines_<k>.cu   explicit instantiations of k_lines, split for parallel
-  inst_x_<k>.cu       and k_xpass, compilation
+  inst_lines_<k>.cu   explicit instantiations of k_lines, k_xpass and
+  inst_x_<k>.cu       k_ypass, split for parallel compilation (the y files
+  inst_y_<k>.cu       keep scalar complex adds: DW_PAIRED_ADDS 0)
 
 A length N is supported when it factors into at most three radices <= 16
 (7-smooth).  The radix list is chosen to minimise the threads per line
 (N / smallest radix), then the number of stages, then the spread.
-Run: python gen_plans.py [--max 4096] [--parts 8]
+Run: python gen_plans.py [--max 4096] [--parts 16]  (the committed files use 16 parts)
 """
 from __future__ import annotations
 
