@@ -542,8 +542,8 @@ def main():
             if k:
                 roof["traffic"] = k["traffic_over_algorithmic"] * dom["bytes_per_launch"]
                 roof["traffic_source"] = (f"ncu dram__bytes_read.sum + dram__bytes_write.sum on "
-                                          f"{tr['capture']['workload']} ({k['dram_bytes_per_launch']:.4g} B per "
-                                          f"launch), scaled by algorithmic bytes")
+                                          f"{k.get('workload', tr['capture']['workload'])} "
+                                          f"({k['dram_bytes_per_launch']:.4g} B per launch), scaled by algorithmic bytes")
     kernels = sorted(
         ({"name": s["name"], "launches": s["launches"], "ms": round(s["ms"], 3),
           "bytes_per_launch": s["bytes_per_launch"],
