@@ -197,3 +197,21 @@ def test_lp_start_port_equals_reference(shape, method):
     b = po.deconvolve(im, psf, method=method, n_iter=3, start=po.START_LP, impl="reference")
     np.testing.assert_array_equal(a.out, b.out)
     np.testing.assert_array_equal(a.trace, b.trace)
+
+
+@need_ref
+@pytest.mark.parametrize("shape,psf_shape,bq", [
+    ((9, 22, 20), (5, 7, 9), 1),     # job 25 x 26 x 12: odd x
+    ((37, 40, 30), (11, 9, 9), 0),   # z period 37 (prime)
+    ((20, 33, 44), (21, 15, 13), 0), # x 44, y 33
+    ((12, 26, 31), (7, 9, 11), 1),   # job 37 x 31 x 16
+])
+def test_port_matches_reference_periodic_sizes(shape, psf_shape, bq):
+    """The sizes the GPU runs with periodic margins: the restatement equals
+    the reference at the reference's own (exact) job size, bit for bit."""
+    im, psf = small_case(seed=6, shape=shape, psf_shape=psf_shape)
+    for m in ("shb", "rl"):
+        a = po.deconvolve(im, psf, method=m, n_iter=5, border_quality=bq, impl="port", threads=1)
+        b = po.deconvolve(im, psf, method=m, n_iter=5, border_quality=bq, impl="reference", threads=1)
+        np.testing.assert_array_equal(a.trace, b.trace)
+        np.testing.assert_array_equal(a.out, b.out)
