@@ -29,6 +29,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -41,8 +42,9 @@ WORKLOAD = "shb-2048x2048x60"
 SMALL = "shb-256x256x40"
 PROFILE_CASE = "shb-1024x1024x20"  # hardware-counter captures (profiles/)
 ITERS = 50
-# generated inputs are cached between runs on one machine (kept out of git)
-CACHE = os.environ.get("DWCU_INPUT_CACHE", os.path.join(ROOT, "_cache"))
+# generated inputs are cached between runs on one machine, outside the
+# repository (a 2048 x 2048 x 60 image is about 1 GB)
+CACHE = os.environ.get("DWCU_INPUT_CACHE", os.path.join(tempfile.gettempdir(), "dwcu_input_cache"))
 
 
 def log(*a):

@@ -1383,8 +1383,9 @@ static int fft3d(const float *d_in, long long M, long long N, long long P, float
     DeviceCtx *ctx = nullptr;
     TRY(get_ctx(device, &ctx));
     CU(cudaSetDevice(device));
-    dwcu_job jj;
+    dwcu_job jj{};
     dwcu_job *j = &jj;
+    dwcu_opts_init(&j->s);
     Geometry &g = j->g;
     g.M = M; g.N = N; g.P = P; g.pM = g.pN = g.pP = 1;
     g.wM = g.X = M; g.wN = g.Y = N; g.wP = g.Z = P;
@@ -1482,8 +1483,9 @@ static_assert(sizeof(JobScalars) <= 256, "noalloc.cu reserves 256 bytes for the 
 int fft3d_r2c_scratch(const float *d_in, long long M, long long N, long long P, float *d_out, cudaStream_t stream,
                       float2 *S, float *real, JobScalars *sc, const float2 *const tw[4])
 {
-    dwcu_job jj;
+    dwcu_job jj{};
     dwcu_job *j = &jj;
+    dwcu_opts_init(&j->s);
     Geometry &g = j->g;
     g.M = M; g.N = N; g.P = P; g.pM = g.pN = g.pP = 1;
     g.wM = g.X = M; g.wN = g.Y = N; g.wP = g.Z = P;

@@ -58,6 +58,22 @@ int fail(int code, const char *msg)
     return code;
 }
 
+// restores the caller's current device on every return path
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() { if (cudaGetDevice(&prev) != cudaSuccess) { cudaGetLastError(); prev = -1; } }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+// work already queued on the shared work space must finish before the lock
+// is released, whatever went wrong after it was queued
+int fail_drained(cudaStream_t st, int code, const char *msg)
+{
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    return fail(code, msg);
+}
+
 // the twiddle table exp(-2 pi i m / n) of the engine (engine.cu computes it
 // on the host in double); this file is compiled without FMA contraction, so
 // the device evaluates the same double operations and rounds to the same floats
@@ -88,6 +104,7 @@ extern "C" int dwcu_fft_r2c_noalloc(const float *d_in, int64_t M, int64_t N, int
                  (long long) M, (long long) N, (long long) P, need, kScratchBytes);
         return fail(DWCU_ERROR_INVALID_VALUE, msg);
     }
+    DeviceGuard restore;
     std::lock_guard<std::mutex> lk(g_mu[device]);
     if (cudaSetDevice(device) != cudaSuccess) {
         cudaGetLastError();
@@ -103,10 +120,10 @@ extern "C" int dwcu_fft_r2c_noalloc(const float *d_in, int64_t M, int64_t N, int
         g_addr[device] = p;
     }
     char *base = (char *) g_addr[device];
-    cudaStream_t st = (cudaStream_t) stream;
+    cudaStream_t st = stream ? (cudaStream_t) stream : cudaStreamPerThread;
     // spectrum, staged input, scalars: cleared; twiddle tables after them
     if (cudaMemsetAsync(base, 0, spec + real + 256, st) != cudaSuccess)
-        return fail(DWCU_ERROR_CUDA, "clearing the work space failed");
+        return fail_drained(st, DWCU_ERROR_CUDA, "clearing the work space failed");
     const float2 *tw[4];
     size_t off = spec + real + 256;
     for (int i = 0; i < 4; ++i) {
@@ -114,7 +131,7 @@ extern "C" int dwcu_fft_r2c_noalloc(const float *d_in, int64_t M, int64_t N, int
         const int blocks = (int) ((lens[i] + 255) / 256);
         k_twiddle_table<<<blocks, 256, 0, st>>>(t, lens[i]);
         dwcu::record_launch();
-        if (cudaGetLastError() != cudaSuccess) return fail(DWCU_ERROR_CUDA, "twiddle launch failed");
+        if (cudaGetLastError() != cudaSuccess) return fail_drained(st, DWCU_ERROR_CUDA, "twiddle launch failed");
         tw[i] = t;
         off += up256(sizeof(float2) * (size_t) lens[i]);
     }

@@ -274,7 +274,10 @@ int dwcu_fft_c2r(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_ou
  * than the work space are rejected with DWCU_ERROR_INVALID_VALUE.  The first
  * call on a device does one-time setup (symbol lookup, kernel attributes).
  * Calls on one device share the work space: they are serialised by a lock
- * and each returns after its stream has drained. */
+ * and each returns after its stream has drained.  A NULL stream means the
+ * calling thread's default stream (cudaStreamPerThread); pass a stream of
+ * your own to keep the transform beside other work.  The caller's current
+ * device is left as it was. */
 int dwcu_fft_r2c_noalloc(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_out, int32_t device,
                          void *stream);
 
