@@ -11,6 +11,16 @@ Small fixtures store inputs and full outputs.  The 256 x 256 x 40 fixture
 (--config1, a few minutes of CPU) stores the I-divergence trace, per-plane
 sums and a seeded sample of 65536 output voxels; the inputs are regenerated
 from their seeds by deconwolf_b200.synthetic.
+
+--config1-fp64 (a few minutes) runs the same 256 x 256 x 40 job through the
+reference build and through the FP64 restatement (oracle/fp64.py) and stores
+the FP64 result at the same sampled voxels, its trace, norm and sketch
+(tests/helpers.sketch), the reference output's sketch and the reference's
+exact relative L2 distance to the FP64 result.
+
+--config2 (about 40 minutes on 8 cores, ~35 GB of RAM) runs the reference's
+SHB for 50 iterations on the 2048 x 2048 x 60 workload and stores its trace,
+plane sums, norm, 262144 sampled voxels and a sketch of the whole output.
 """
 from __future__ import annotations
 
@@ -63,15 +73,67 @@ def config1():
         threads=np.int64(os.cpu_count()))
 
 
+def config1_fp64():
+    from deconwolf_b200 import synthetic
+    from oracle.fp64 import deconvolve_fp64
+    from tests.helpers import sketch
+    name = "shb-256x256x40"
+    im, psf = synthetic.config_inputs(name)
+    r = po.deconvolve(im, psf, method="shb", n_iter=50, impl="reference", threads=os.cpu_count())
+    t = time.time()
+    f = deconvolve_fp64(im, psf, method="shb", n_iter=50)
+    print("FP64 SHB 256x256x40, 50 it:", time.time() - t, "s")
+    idx = sample_index(im.shape, 65536)
+    ref = r.out.astype(np.float64)
+    np.savez_compressed(
+        os.path.join(HERE, "config1_fp64.npz"),
+        sample_idx=idx, fp64_sample=f.out.reshape(-1)[idx], fp64_trace=f.trace,
+        fp64_norm=np.float64(np.linalg.norm(f.out)), fp64_sketch=sketch(f.out), ref_sketch=sketch(ref),
+        ref_norm=np.float64(np.linalg.norm(ref)),
+        ref_rel_l2_fp64=np.float64(np.linalg.norm(ref - f.out) / np.linalg.norm(f.out)),
+        ref_trace_rel_fp64=np.float64(np.max(np.abs(r.trace - f.trace) / f.trace)))
+    print("reference vs FP64: rel L2", np.linalg.norm(ref - f.out) / np.linalg.norm(f.out))
+
+
+def config2():
+    from deconwolf_b200 import synthetic
+    from tests.helpers import sketch
+    name = "shb-2048x2048x60"
+    t = time.time()
+    im, psf = synthetic.config_inputs(name)
+    print("inputs", time.time() - t, "s", flush=True)
+    t = time.time()
+    r = po.deconvolve(im, psf, method="shb", n_iter=50, impl="reference", threads=os.cpu_count())
+    print("reference SHB 2048x2048x60, 50 it:", time.time() - t, "s; loop", r.loop_seconds, flush=True)
+    idx = np.sort(sample_index(im.shape, 262144))
+    out = r.out
+    np.savez_compressed(
+        os.path.join(HERE, "config2_shb50.npz"),
+        trace=r.trace, plane_sums=out.astype(np.float64).sum(axis=(1, 2)), sample_idx=idx,
+        sample_val=out.reshape(-1)[idx], norm=np.float64(np.linalg.norm(out.astype(np.float64))),
+        sketch=sketch(out), image_sum=np.float64(im.astype(np.float64).sum()),
+        psf_sum=np.float64(psf.astype(np.float64).sum()), image_sample=im.reshape(-1)[idx],
+        bg=np.float32(r.bg), loop_seconds=np.float64(r.loop_seconds), threads=np.int64(os.cpu_count()))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--config1", action="store_true")
+    ap.add_argument("--config1-fp64", action="store_true")
+    ap.add_argument("--config2", action="store_true")
+    ap.add_argument("--no-small", action="store_true")
     a = ap.parse_args()
-    small("small_shb", (11, 40, 37), (7, 9, 11), seed=11, method="shb", n_iter=20)
-    small("small_rl", (11, 40, 37), (7, 9, 11), seed=12, method="rl", n_iter=20)
-    small("small_shb_rel", (8, 33, 30), (5, 9, 9), seed=13, method="shb", iter_type=po.ITER_REL, err_rel=0.001)
+    if not a.no_small:
+        small("small_shb", (11, 40, 37), (7, 9, 11), seed=11, method="shb", n_iter=20)
+        small("small_rl", (11, 40, 37), (7, 9, 11), seed=12, method="rl", n_iter=20)
+        small("small_shb_rel", (8, 33, 30), (5, 9, 9), seed=13, method="shb", iter_type=po.ITER_REL,
+              err_rel=0.001)
     if a.config1:
         config1()
+    if a.config1_fp64:
+        config1_fp64()
+    if a.config2:
+        config2()
 
 
 if __name__ == "__main__":

@@ -36,3 +36,45 @@ def rel_l2(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+# ---------------------------------------------------------------- sketches
+# A full-volume check for outputs too large to store as a fixture: k rows of
+# pseudo-random +-1 signs (a seeded integer hash of the voxel index, the same
+# on every device) projected onto the flattened volume, summed in float64.
+# For any vector d, ||S d||^2 / k estimates ||d||^2 without bias (relative
+# spread about sqrt(2 / k)), so ||S a - S b|| / (sqrt(k) ||b||) estimates the
+# relative L2 distance of a and b over every voxel.
+_P31 = 2147483647
+SKETCH_ROWS = 32
+
+
+def _sketch_consts(k):
+    rng = np.random.default_rng(20240611)
+    return (rng.integers(1, _P31, k), rng.integers(0, _P31, k), rng.integers(0, _P31, k))
+
+
+def sketch(v, k: int = SKETCH_ROWS, device: str = "cpu", chunk: int = 1 << 24) -> np.ndarray:
+    """S v for the flattened volume v (NumPy or torch), as float64[k]."""
+    import torch
+    t = v if isinstance(v, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(v))
+    t = t.reshape(-1).to(device)
+    A, B, C = _sketch_consts(k)
+    out = np.zeros(k, dtype=np.float64)
+    n = t.numel()
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        i = torch.arange(s, e, dtype=torch.int64, device=device)
+        vv = t[s:e].to(torch.float64)
+        for j in range(k):
+            h = (i * int(A[j]) + int(B[j])) % _P31       # < 2^62: no overflow
+            h = (h * h + int(C[j])) % _P31
+            sgn = ((h >> 16) & 1).to(torch.float64) * 2 - 1
+            out[j] += float((sgn * vv).sum())
+    return out
+
+
+def sketch_rel_l2(sk_a, sk_b, norm_b: float) -> float:
+    """Estimated relative L2 distance of a to b from their sketches."""
+    k = len(sk_a)
+    return float(np.linalg.norm(np.asarray(sk_a) - np.asarray(sk_b)) / (np.sqrt(k) * norm_b))

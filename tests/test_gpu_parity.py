@@ -163,6 +163,35 @@ def test_config1_golden():
     assert abs(np.linalg.norm(g.out.astype(np.float64)) / d["norm"] - 1) < OUT_TOL
 
 
+def test_config2_golden():
+    """2048 x 2048 x 60, Born-Wolf 181 x 181 x 119 PSF, SHB 50 iterations
+    (job 2228 x 2228 x 178, padded here to 2240 x 2240 x 180) against the
+    reference's own output: the full I-divergence trace, every plane sum, the
+    norm, 262144 sampled voxels and the relative L2 distance over the whole
+    volume estimated from a 32-row sketch."""
+    f = os.path.join(os.path.dirname(__file__), "golden", "config2_shb50.npz")
+    if not os.path.exists(f):
+        pytest.skip("config2 fixture not generated")
+    from deconwolf_b200 import synthetic
+    from tests.helpers import sketch, sketch_rel_l2
+    d = np.load(f)
+    im, psf = synthetic.config_inputs("shb-2048x2048x60")
+    idx = d["sample_idx"]
+    np.testing.assert_array_equal(im.reshape(-1)[idx], d["image_sample"])  # same inputs as the fixture
+    assert abs(float(im.astype(np.float64).sum()) - float(d["image_sum"])) == 0
+    g = dw.run_method(im, psf, method="shb", n_iter=50)
+    assert g.work == (2240, 2240, 180)
+    assert trace_err(g.trace, d["trace"]) < TRACE_TOL
+    assert rel_l2(g.out.reshape(-1)[idx], d["sample_val"]) < OUT_TOL
+    assert rel_l2(g.out.astype(np.float64).sum(axis=(1, 2)), d["plane_sums"]) < OUT_TOL
+    assert abs(np.linalg.norm(g.out.astype(np.float64)) / d["norm"] - 1) < OUT_TOL
+    est = sketch_rel_l2(sketch(g.out, device="cuda"), d["sketch"], float(d["norm"]))
+    print(f"\nconfig 2: relative L2 to the reference over the volume (sketch) {est:.3e}, "
+          f"on samples {rel_l2(g.out.reshape(-1)[idx], d['sample_val']):.3e}, "
+          f"trace {trace_err(g.trace, d['trace']):.2e}")
+    assert est < OUT_TOL
+
+
 def test_deterministic():
     im, psf = case_inputs(seed=7, shape=(12, 40, 36), psf_shape=(7, 9, 9))
     a = dw.run_method(im, psf, n_iter=15)
