@@ -126,7 +126,14 @@ EXPORTS = [
     "dwcu_tiling_create", "dwcu_deconvolve_tiled", "dwcu_fft_r2c_noalloc", "dwcu_server_create",
     "dwcu_server_submit", "dwcu_server_wait", "dwcu_server_cancel", "dwcu_server_get_stats",
     "dwcu_server_destroy", "dwcu_tile_blend", "dwcu_release_cache",
+    "dwcu_tune_set_mode", "dwcu_tune_get_mode", "dwcu_tune_select", "dwcu_tune_plan_count",
+    "dwcu_tune_plan_info", "dwcu_tune_force", "dwcu_tune_run", "dwcu_tune_query", "dwcu_tune_clear",
+    "dwcu_tune_export", "dwcu_tune_import",
 ]
+
+# pass kinds of the autotuner (dwcu.h)
+PLAN_LINES, PLAN_Y, PLAN_X = 0, 1, 2
+TUNE_OFF, TUNE_MEASURE = 0, 1
 
 _lib = None
 
@@ -194,6 +201,23 @@ def lib() -> ctypes.CDLL:
     L.dwcu_server_destroy.restype = None
     L.dwcu_tile_blend.argtypes = [vp, i64, i64, i64, ctypes.POINTER(Tile), i32, i32, vp, ctypes.c_float, i32, vp]
     L.dwcu_tile_blend.restype = ctypes.c_int
+    f32p = ctypes.POINTER(ctypes.c_float)
+    i32p = ctypes.POINTER(i32)
+    L.dwcu_tune_set_mode.argtypes = [i32]
+    L.dwcu_tune_get_mode.argtypes = [i32p]
+    L.dwcu_tune_select.argtypes = [f32p, i32, ctypes.c_float, i32p]
+    L.dwcu_tune_plan_count.argtypes = [i32, i32, i32p]
+    L.dwcu_tune_plan_info.argtypes = [i32, i32, i32, i32p, i32p]
+    L.dwcu_tune_force.argtypes = [i32, i32, i32]
+    L.dwcu_tune_run.argtypes = [i32, i32, i32]
+    L.dwcu_tune_query.argtypes = [i32, i32, i32, i32p, f32p, i32, i32p]
+    L.dwcu_tune_clear.argtypes = []
+    L.dwcu_tune_export.argtypes = [ctypes.c_char_p]
+    L.dwcu_tune_import.argtypes = [ctypes.c_char_p]
+    for fn in (L.dwcu_tune_set_mode, L.dwcu_tune_get_mode, L.dwcu_tune_select, L.dwcu_tune_plan_count,
+               L.dwcu_tune_plan_info, L.dwcu_tune_force, L.dwcu_tune_run, L.dwcu_tune_query, L.dwcu_tune_clear,
+               L.dwcu_tune_export, L.dwcu_tune_import):
+        fn.restype = ctypes.c_int
     L.dwcu_batch_run.argtypes = [ctypes.POINTER(vp), i32, vp]
     L.dwcu_batch_run.restype = ctypes.c_int
     L.dwcu_psf_prepare.argtypes = [vp, i64, i64, i64, i64, i64, i64, i32, ctypes.c_float, vp,
@@ -561,3 +585,61 @@ def deconvolve(image: np.ndarray, psf: np.ndarray, iterations: int, bq: int = 2,
         raise ValueError("The image has too low intensity, can not continue!")  # dw.c:2711-2721
     return dw_run(im, psf, offset=offset, method=method, n_iter=iterations, iter_type=ITER_FIXED,
                   border_quality=bq, verbosity=verbose, device=device)
+
+
+# ---------------------------------------------------------------- autotuning
+
+def tune_select(times_ms, margin: float = 0.02) -> int:
+    """The autotuner's selection rule on candidate times (host logic)."""
+    arr = (ctypes.c_float * len(times_ms))(*times_ms)
+    out = ctypes.c_int32()
+    _check(lib().dwcu_tune_select(arr, len(times_ms), margin, ctypes.byref(out)))
+    return out.value
+
+
+def tune_plans(kind: int, n: int):
+    """[(radices, tile), ...] of the candidate plans of a length (candidate 0 first)."""
+    cnt = ctypes.c_int32()
+    _check(lib().dwcu_tune_plan_count(kind, n, ctypes.byref(cnt)))
+    out = []
+    for c in range(cnt.value):
+        rad = (ctypes.c_int32 * 3)()
+        tile = ctypes.c_int32()
+        _check(lib().dwcu_tune_plan_info(kind, n, c, rad, ctypes.byref(tile)))
+        out.append((tuple(int(r) for r in rad if r > 1) or (1,), int(tile.value)))
+    return out
+
+
+def tune_force(kind: int, n: int, cand: int) -> None:
+    """Use candidate ``cand`` for this length from now on (-1: measure again)."""
+    _check(lib().dwcu_tune_force(kind, n, cand))
+
+
+def tune_run(kind: int, n: int, device: int = 0) -> None:
+    """Time the candidates of one length now (if not recorded yet)."""
+    _check(lib().dwcu_tune_run(device, kind, n))
+
+
+def tune_query(kind: int, n: int, device: int = 0):
+    """(chosen candidate or -1, [ms per candidate])."""
+    cand = ctypes.c_int32()
+    ms = (ctypes.c_float * 16)()
+    k = ctypes.c_int32()
+    _check(lib().dwcu_tune_query(device, kind, n, ctypes.byref(cand), ms, 16, ctypes.byref(k)))
+    return cand.value, [float(ms[i]) for i in range(k.value)]
+
+
+def tune_set_mode(mode: int) -> None:
+    _check(lib().dwcu_tune_set_mode(mode))
+
+
+def tune_clear() -> None:
+    _check(lib().dwcu_tune_clear())
+
+
+def tune_export(path: str) -> None:
+    _check(lib().dwcu_tune_export(os.fsencode(path)))
+
+
+def tune_import(path: str) -> None:
+    _check(lib().dwcu_tune_import(os.fsencode(path)))

@@ -82,6 +82,7 @@ struct ProfClass {
 };
 static std::mutex g_prof_mu;
 static bool g_prof_on = false;
+static thread_local bool g_tuning = false;  // the autotuner's launches are not profiled
 static std::vector<ProfRec> g_prof_recs;
 static std::vector<cudaEvent_t> g_prof_pool;
 static std::vector<ProfClass> g_prof_classes;
@@ -114,7 +115,7 @@ struct ProfScope {
     ProfScope(const char *name, double bytes, cudaStream_t s)
     {
         std::lock_guard<std::mutex> lk(g_prof_mu);
-        if (!g_prof_on) return;
+        if (!g_prof_on || g_tuning) return;
         on = true;
         st = s;
         rec.cls = prof_class(name, bytes);
@@ -200,6 +201,34 @@ static const YPlan *find_y(int n)
         if (p.n == n) return &p;
     return nullptr;
 }
+
+// candidate `cand` of a length (find_*: candidate 0, listed first)
+static const LinesPlan *lines_plan(int n, int cand)
+{
+    for (const auto &p : kLinesPlans)
+        if (p.n == n && p.cand == cand) return &p;
+    return nullptr;
+}
+static const XPlan *x_plan(int n, int cand)
+{
+    for (const auto &p : kXPlans)
+        if (p.n == n && p.cand == cand) return &p;
+    return nullptr;
+}
+static const YPlan *y_plan(int n, int cand)
+{
+    for (const auto &p : kYPlans)
+        if (p.n == n && p.cand == cand) return &p;
+    return nullptr;
+}
+
+// the autotuner's table (tune.cu)
+int tune_plan_count(int kind, int n);
+int tune_mode();
+float tune_margin();
+int tune_lookup(int device, int kind, int n);
+void tune_record(int device, int kind, int n, const std::vector<float> &ms, int cand);
+int tune_select_idx(const float *ms, int n, float margin);
 
 static int make_geometry(long long M, long long N, long long P, long long pM, long long pN, long long pP, int bq,
                          Geometry &g)
@@ -817,6 +846,216 @@ static int alloc_job(dwcu_job *j)
     return DWCU_SUCCESS;
 }
 
+// ------------------------------------------------------------ autotuning
+//
+// tune_measure times the candidate plans of one transform length and pass
+// kind (tune.cu keeps the choices).  Each candidate runs the pass it would
+// run in an iteration on a synthetic volume of about kTuneElems complex
+// elements: the z pass's convolve mode (lines), the persistent y pass in both
+// directions (y), the SHB ratio and update x passes (x); one warm-up launch,
+// then kTuneReps launches between CUDA events, on a stream of the tuner's
+// own.  The volume is filled so that the ratio pass takes its usual branches
+// (a positive image, a large constant term in every spectrum row, so that
+// the blurred estimate is positive).  The scratch memory (a few hundred MB)
+// is allocated for the measurement and freed after it.
+
+static std::mutex g_tune_mu;
+constexpr long long kTuneElems = 8LL << 20;  // complex elements of the synthetic spectrum (64 MB)
+constexpr int kTuneReps = 4;
+
+__device__ __forceinline__ unsigned tune_hash(unsigned long long i, unsigned seed)
+{
+    unsigned h = (unsigned) i * 2654435761u ^ (unsigned) (i >> 32) ^ seed;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    return h;
+}
+
+__global__ void k_tune_fill_real(float *p, long long n, float base, float amp, unsigned seed)
+{
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x)
+        p[i] = base + amp * (float) (tune_hash((unsigned long long) i, seed) & 0xffffu) * (1.f / 65536.f);
+}
+
+// blocked spectrum: a large real term at kx = 0 of every row, small noise elsewhere
+__global__ void k_tune_fill_spec(float2 *S, long long n, int Y, int nkb, float dc, unsigned seed)
+{
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
+        const int ki = (int) (i % KB);
+        const int kb = (int) ((i / KB / Y) % nkb);
+        const unsigned h = tune_hash((unsigned long long) i, seed);
+        S[i] = (kb == 0 && ki == 0) ? make_float2(dc, 0.f)
+                                    : make_float2((float) (h & 0xffffu) * (1.f / 65536.f) - 0.5f,
+                                                  (float) (h >> 16) * (1.f / 65536.f) - 0.5f);
+    }
+}
+
+static int tune_measure(DeviceCtx *ctx, int kind, int n, std::vector<float> &ms)
+{
+    const int cnt = (int) ms.size();
+    std::fill(ms.begin(), ms.end(), -1.f);
+    // a synthetic job of the pass's length, without OTF or weights set-up
+    dwcu_job jj{};
+    dwcu_opts_init(&jj.s);
+    jj.s.device = ctx->device;
+    jj.ctx = ctx;
+    Geometry &g = jj.g;
+    size_t spec = 0, real = 0, gbytes = 0;
+    long long rows = 0;
+    if (kind == DWCU_PLAN_LINES) {
+        // z lines of length n over planes of 128 complex columns x Y rows
+        g.X = 254; g.NKB = 32; g.Z = n;
+        g.Y = std::max<long long>(1, kTuneElems / (n * g.NKB * KB));
+        spec = sizeof(float2) * (size_t) (g.spec_elems() + 8 * KB);
+    } else if (kind == DWCU_PLAN_Y) {
+        g.X = 254; g.NKB = 32; g.Y = n;
+        g.Z = std::max<long long>(1, kTuneElems / (n * g.NKB * KB));
+        spec = sizeof(float2) * (size_t) (g.spec_elems() + 8 * KB);
+    } else {
+        // x rows of length 2n, every row and column inside the image
+        const XPlan *p0 = x_plan(n, 0);
+        if (!p0) return fail(DWCU_ERROR_UNSUPPORTED, "no x plan of length %d", n);
+        g.X = 2LL * n; g.XP = (g.X + 3) & ~3LL; g.GP = g.XP;
+        g.NKB = (n + 1 + KB - 1) / KB;
+        rows = std::max<long long>(p0->R, kTuneElems / (g.NKB * KB));
+        rows = (rows + p0->R - 1) / p0->R * p0->R;
+        g.Y = rows; g.Z = 1;
+        g.M = g.X; g.N = g.Y; g.P = 1;
+        g.xp = p0;
+        spec = sizeof(float2) * (size_t) (g.spec_elems() + 8 * KB);
+        real = sizeof(float) * (size_t) (g.real_elems() + g.XP);
+        gbytes = real;
+    }
+    g.wM = g.X; g.wN = g.Y; g.wP = g.Z;
+    const long long nxb = kind == DWCU_PLAN_X ? x_blocks(g) : 0;
+    size_t off = 0;
+    auto take = [&](size_t b) { size_t o = off; off += align256(b); return o; };
+    const size_t o_S = take(spec), o_K = kind == DWCU_PLAN_LINES ? take(spec) : 0;
+    const size_t o_g = take(gbytes), o_xa = take(real), o_xb = take(real), o_W = take(real), o_xd = take(real);
+    const size_t o_part = take(sizeof(double) * (size_t) (nxb + 1));
+    const size_t o_sc = take(sizeof(JobScalars));
+    char *base = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = DWCU_SUCCESS;
+    if (cudaMalloc(&base, off) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DWCU_ERROR_OUT_OF_MEMORY, "no device memory for the tuning volume");
+    }
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess)
+        rc = fail(DWCU_ERROR_CUDA, "tuning stream or events could not be created");
+    jj.stream = st;
+    jj.S = (float2 *) (base + o_S);
+    jj.K = kind == DWCU_PLAN_LINES ? (float2 *) (base + o_K) : nullptr;
+    jj.sc = (JobScalars *) (base + o_sc);
+    if (kind == DWCU_PLAN_X) {
+        jj.gimg = (float *) (base + o_g);
+        jj.xa = (float *) (base + o_xa);
+        jj.xb = (float *) (base + o_xb);
+        jj.W = (float *) (base + o_W);
+        jj.partial = (double *) (base + o_part);
+        jj.nxb = nxb;
+    }
+    if (rc == DWCU_SUCCESS) rc = get_twiddles(ctx, kind == DWCU_PLAN_X ? g.X : n, kind == DWCU_PLAN_X ? &jj.tw_x : kind == DWCU_PLAN_Y ? &jj.tw_y : &jj.tw_z);
+    if (rc == DWCU_SUCCESS && kind == DWCU_PLAN_X) rc = get_twiddles(ctx, n, &jj.tw_l);
+    if (rc == DWCU_SUCCESS) {
+        const long long ns = g.spec_elems();
+        k_tune_fill_spec<<<592, 256, 0, st>>>(jj.S, ns, (int) g.Y, (int) g.NKB, 50.f * (float) g.X, 1u);
+        if (jj.K) k_tune_fill_spec<<<592, 256, 0, st>>>(jj.K, ns, (int) g.Y, (int) g.NKB, 1.f, 2u);
+        if (kind == DWCU_PLAN_X) {
+            const long long nr = g.real_elems();
+            k_tune_fill_real<<<592, 256, 0, st>>>(jj.gimg, nr, 50.f, 100.f, 3u);
+            k_tune_fill_real<<<592, 256, 0, st>>>(jj.xa, nr, 20.f, 10.f, 4u);
+            k_tune_fill_real<<<592, 256, 0, st>>>(jj.xb, nr, 20.f, 10.f, 5u);
+            k_tune_fill_real<<<592, 256, 0, st>>>(jj.W, nr, 0.5f, 1.f, 6u);
+        }
+        if (cudaMemsetAsync(jj.sc, 0, sizeof(JobScalars), st) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+            rc = fail(DWCU_ERROR_CUDA, "filling the tuning volume failed");
+    }
+    g_tuning = true;
+    auto run_pass = [&]() -> int {
+        if (kind == DWCU_PLAN_LINES) return pass_z(&jj, LINES_CONV, jj.S);
+        if (kind == DWCU_PLAN_Y) {
+            TRY(pass_y(&jj, LINES_FWD, jj.S));
+            return pass_y(&jj, LINES_INV, jj.S);
+        }
+        TRY(pass_x(&jj, XOP_RATIO_SHB, 1, jj.S, nullptr, nullptr, nullptr, 0, 0, jj.nxb));
+        return pass_x(&jj, XOP_UPDATE_SHB, 1, jj.S, jj.xa, jj.xb, (float *) (base + o_xd), 0.5, 0.6);
+    };
+    for (int c = 0; c < cnt && rc == DWCU_SUCCESS; ++c) {
+        if (kind == DWCU_PLAN_LINES) g.zp = lines_plan(n, c);
+        else if (kind == DWCU_PLAN_Y) g.ytp = y_plan(n, c);
+        else g.xp = x_plan(n, c);
+        if ((kind == DWCU_PLAN_LINES && !g.zp) || (kind == DWCU_PLAN_Y && !g.ytp) || (kind == DWCU_PLAN_X && !g.xp)) {
+            rc = fail(DWCU_ERROR_INTERNAL, "missing tuning candidate %d of length %d", c, n);
+            break;
+        }
+        rc = run_pass();  // warm-up (also sets the kernel's shared-memory attribute)
+        if (rc == DWCU_SUCCESS && cudaEventRecord(e0, st) != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "event record failed");
+        for (int r = 0; r < kTuneReps && rc == DWCU_SUCCESS; ++r) rc = run_pass();
+        if (rc == DWCU_SUCCESS && cudaEventRecord(e1, st) != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "event record failed");
+        float t = 0.f;
+        if (rc == DWCU_SUCCESS && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
+            rc = fail(DWCU_ERROR_CUDA, "timing a tuning candidate failed");
+        if (rc == DWCU_SUCCESS) ms[(size_t) c] = t / (float) kTuneReps;
+    }
+    g_tuning = false;
+    // a bounded wait that gave up makes the measurement worthless
+    JobScalars hs{};
+    if (st) cudaStreamSynchronize(st);
+    if (rc == DWCU_SUCCESS && cudaMemcpy(&hs, jj.sc, sizeof hs, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = fail(DWCU_ERROR_CUDA, "reading the tuning flags failed");
+    if (rc == DWCU_SUCCESS && (hs.flags & ~0xff))
+        rc = fail(DWCU_ERROR_TIMEOUT, "a bounded wait gave up while tuning length %d", n);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    cudaFree(base);
+    return rc;
+}
+
+// the recorded choice of (device, kind, n), measured now if there is none
+// and tuning is on; 0 (the heuristic plan) when the measurement fails
+static int tuned_choice(DeviceCtx *ctx, int kind, int n, int *rc_out = nullptr)
+{
+    const int cnt = tune_plan_count(kind, n);
+    if (cnt <= 1) return 0;
+    int c = tune_lookup(ctx->device, kind, n);
+    if (c >= 0 && c < cnt) return c;
+    if (tune_mode() == DWCU_TUNE_OFF && !rc_out) return 0;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    c = tune_lookup(ctx->device, kind, n);  // measured meanwhile by another thread
+    if (c >= 0 && c < cnt) return c;
+    std::vector<float> ms((size_t) cnt, -1.f);
+    const std::string saved = g_last_error;
+    const int rc = tune_measure(ctx, kind, n, ms);
+    if (rc_out) *rc_out = rc;
+    if (rc != DWCU_SUCCESS) {
+        cudaGetLastError();
+        if (!rc_out) g_last_error = saved;
+        return 0;
+    }
+    c = tune_select_idx(ms.data(), cnt, tune_margin());
+    tune_record(ctx->device, kind, n, ms, c);
+    return c;
+}
+
+// the geometry's plans: candidate 0 from make_geometry, replaced by the
+// tuned choice of each pass's length
+static void tune_geometry(DeviceCtx *ctx, Geometry &g)
+{
+    const int nx = (int) (g.X / 2);
+    if (const XPlan *p = x_plan(nx, tuned_choice(ctx, DWCU_PLAN_X, nx))) g.xp = p;
+    if (g.ytp) {
+        if (const YPlan *p = y_plan((int) g.Y, tuned_choice(ctx, DWCU_PLAN_Y, (int) g.Y))) g.ytp = p;
+    } else if (g.yp) {
+        if (const LinesPlan *p = lines_plan((int) g.Y, tuned_choice(ctx, DWCU_PLAN_LINES, (int) g.Y))) g.yp = p;
+    }
+    if (const LinesPlan *p = lines_plan((int) g.Z, tuned_choice(ctx, DWCU_PLAN_LINES, (int) g.Z))) g.zp = p;
+}
+
 static long long job_bytes_estimate(const Geometry &g, const dwcu_opts &s)
 {
     const long long R = 4LL * g.real_elems();
@@ -851,6 +1090,7 @@ static int job_create(long long M, long long N, long long P, long long pM, long 
     DeviceCtx *ctx = nullptr;
     TRY(get_ctx(s->device, &ctx));
     CU(cudaSetDevice(s->device));
+    tune_geometry(ctx, g);
     dwcu_job *j = new dwcu_job();
     j->s = *s;
     j->g = g;
@@ -1053,10 +1293,11 @@ static int job_step_impl(dwcu_job *j, int nmax, int *remaining)
                 char key[512];
                 const Geometry &gg = j->g;
                 snprintf(key, sizeof key,
-                         "%lld %lld %lld %lld %lld %lld %lld %lld %lld|%d %d %d %d %d %d %d %a|%d %d %d %p %p",
+                         "%lld %lld %lld %lld %lld %lld %lld %lld %lld|%d %d %d %d %d %d %d %a|%d %d %d %p %p|%p %p %p %p",
                          gg.M, gg.N, gg.P, gg.pM, gg.pN, gg.pP, gg.X, gg.Y, gg.Z, j->s.method, j->it.niter,
                          j->s.maxiter, k, j->s.metric, j->s.positivity, j->s.border_quality, (double) j->s.alphamax,
-                         (int) j->spectrum_ready, (int) (j->W != nullptr), (int) prof, (void *) j->xa, (void *) j->xb);
+                         (int) j->spectrum_ready, (int) (j->W != nullptr), (int) prof, (void *) j->xa, (void *) j->xb,
+                         (const void *) gg.xp, (const void *) gg.yp, (const void *) gg.zp, (const void *) gg.ytp);
                 const std::string skey(key);
                 cudaGraphExec_t ex = nullptr;
                 auto hit = j->block->graphs.find(skey);
@@ -1669,6 +1910,18 @@ int64_t dwcu_job_bytes(const dwcu_job *job) { return job ? (int64_t) job->bytes 
 
 const char *dwcu_last_error(void) { return g_last_error.c_str(); }
 int dwcu_abi_version(void) { return DWCU_ABI_VERSION; }
+
+int dwcu_tune_run(int32_t device, int32_t kind, int32_t n)
+{
+    if (kind < DWCU_PLAN_LINES || kind > DWCU_PLAN_X) return fail(DWCU_ERROR_INVALID_VALUE, "bad plan kind");
+    if (tune_plan_count(kind, n) < 1) return fail(DWCU_ERROR_UNSUPPORTED, "no plan of length %d for this pass", n);
+    DeviceCtx *ctx = nullptr;
+    TRY(get_ctx(device, &ctx));
+    CU(cudaSetDevice(device));
+    int rc = DWCU_SUCCESS;
+    tuned_choice(ctx, kind, n, &rc);
+    return rc;
+}
 int dwcu_device_count(void)
 {
     int n = 0;

@@ -9,8 +9,10 @@ Writes, next to this file:
   inst_y_<k>.cu       keep scalar complex adds: DW_PAIRED_ADDS 0)
 
 A length N is supported when it factors into at most three radices <= 16
-(7-smooth).  The radix list is chosen to minimise the threads per line
-(N / smallest radix), then the number of stages, then the spread.
+(7-smooth).  Candidate 0 of a length is the radix list that minimises the
+threads per line (N / smallest radix), then the number of stages, then the
+spread; the other candidates (alternate radix lists, a narrower column
+tile) are for the engine's autotuner, which times them at first use.
 Run: python gen_plans.py [--max 4096] [--parts 16]  (the committed files use 16 parts)
 """
 from __future__ import annotations
@@ -139,6 +141,87 @@ def rad_str(s):
     return f"Rad<{s[0]}, {s[1]}, {s[2]}>"
 
 
+def ranked_splits(n):
+    """Every split of n into at most three radices <= 16, best first by the
+    heuristic of best_split (so ranked_splits(n)[0] == best_split(n))."""
+    if n == 1:
+        return [(1, 1, 1)]
+    cands = set()
+    if n in RADS:
+        cands.add((n, 1, 1))
+    for a in RADS:
+        if n % a:
+            continue
+        b = n // a
+        if b in RADS:
+            cands.add((a, b, 1))
+        for c in RADS:
+            if b % c == 0 and (b // c) in RADS:
+                cands.add((a, c, b // c))
+    best = best_split(n)
+    rest = sorted(cands - {best}, key=lambda s: (tpl_of(n, s), 3 if s[2] > 1 else 2,
+                                                 max(r for r in s if r > 1) - min(r for r in s if r > 1), -s[0], s))
+    return [best] + rest
+
+
+def alternates(n, ok, count):
+    """Up to `count` splits after the best one that pass ok(split), each with a
+    first radix not used by an earlier candidate (the first radix sets the
+    global read pattern and the thread count of the first stage)."""
+    out = []
+    ranked = ranked_splits(n)
+    used = {ranked[0][0]}
+    for s in ranked[1:]:
+        if len(out) == count:
+            break
+        if s[0] in used or not ok(s):
+            continue
+        used.add(s[0])
+        out.append(s)
+    return out
+
+
+# Autotuning candidates per length (the engine times them at first use and
+# keeps the fastest; candidate 0 is the heuristic's choice):
+#   lines (z pass, and the y pass where its tile does not fit): the best
+#     split at its column tile T, the best alternate split, and the best
+#     split with half the column tile
+#   y (persistent 4-line tiles): the best split and up to two alternates
+#   x: the best split; for half lengths >= X_ALT_MIN one alternate split with
+#     the same rows per tile, compiled for the iteration's two families
+#     (ratio and update) only -- the set-up families use candidate 0
+X_ALT_MIN = 96
+
+
+def lines_cands(n):
+    s0 = best_split(n)
+    T0, _ = lines_T(n, s0)
+    out = [(s0, T0)]
+    if n > 1:
+        for s in alternates(n, lambda s: True, 1):
+            out.append((s, lines_T(n, s)[0]))
+        if T0 >= 4:
+            out.append((s0, T0 // 2))
+    return out
+
+
+def y_cands(n):
+    return [best_split(n)] + alternates(n, lambda s: y_fits(n, s), 2)
+
+
+def x_cands(n):
+    s0 = best_split(n)
+    R0, _ = x_R(n, s0)
+    out = [(s0, R0)]
+    if n >= X_ALT_MIN:
+        def ok(s):
+            R, _ = x_R(n, s)
+            return R == R0 and x_smem(n, s, R) <= SMEM_MAX
+        for s in alternates(n, ok, 1):
+            out.append((s, R0))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--max", type=int, default=4096)
@@ -153,43 +236,44 @@ def main():
         keep = {int(v) for v in args.only.split(",")}
         lines_ns = [n for n in lines_ns if n in keep or n == 1]
         x_ns = [n for n in x_ns if n in keep]
+    y_ns = [n for n in lines_ns if n > 1 and y_fits(n, best_split(n))]
 
     hdr = []
     hdr.append("// generated by gen_plans.py -- do not edit")
     hdr.append("#pragma once")
     hdr.append("#include \"passes.cuh\"")
     hdr.append("namespace dwcu {")
-    hdr.append("struct LinesPlan { int n, ra, rb, rc, T, threads; size_t smem; void (*launch)(const LinesArgs &, int, cudaStream_t); };")
-    hdr.append("struct XPlan { int n, ra, rb, rc, R, threads; size_t smem; void (*launch)(const XArgs &, cudaStream_t); };")
-    hdr.append("struct YPlan { int n, ra, rb, rc, threads; size_t smem; void (*launch)(const YArgs &, cudaStream_t); };")
-    y_ns = [n for n in lines_ns if n > 1 and y_fits(n, best_split(n))]
+    hdr.append("// one entry per autotuning candidate of a length, candidates of a length in")
+    hdr.append("// order (cand 0: the generator's heuristic choice)")
+    hdr.append("struct LinesPlan { int n, cand, ra, rb, rc, T, threads; size_t smem; void (*launch)(const LinesArgs &, int, cudaStream_t); };")
+    hdr.append("struct XPlan { int n, cand, ra, rb, rc, R, threads; size_t smem; void (*launch)(const XArgs &, cudaStream_t); };")
+    hdr.append("struct YPlan { int n, cand, ra, rb, rc, threads; size_t smem; void (*launch)(const YArgs &, cudaStream_t); };")
     for n in lines_ns:
-        s = best_split(n)
-        T, _ = lines_T(n, s)
-        hdr.append(f"void launch_lines_{n}(const LinesArgs &, int, cudaStream_t);")
+        for c, _ in enumerate(lines_cands(n)):
+            hdr.append(f"void launch_lines_{n}_{c}(const LinesArgs &, int, cudaStream_t);")
     for n in x_ns:
-        hdr.append(f"void launch_x_{n}(const XArgs &, cudaStream_t);")
+        for c, _ in enumerate(x_cands(n)):
+            hdr.append(f"void launch_x_{n}_{c}(const XArgs &, cudaStream_t);")
     for n in y_ns:
-        hdr.append(f"void launch_y_{n}(const YArgs &, cudaStream_t);")
+        for c, _ in enumerate(y_cands(n)):
+            hdr.append(f"void launch_y_{n}_{c}(const YArgs &, cudaStream_t);")
     hdr.append("static const LinesPlan kLinesPlans[] = {")
     for n in lines_ns:
-        s = best_split(n)
-        T, _ = lines_T(n, s)
-        hdr.append(f"    {{{n}, {s[0]}, {s[1]}, {s[2]}, {T}, LinesCfg<{rad_str(s)}, {T}>::THREADS, "
-                   f"LinesCfg<{rad_str(s)}, {T}>::SMEM_BYTES, launch_lines_{n}}},")
+        for c, (s, T) in enumerate(lines_cands(n)):
+            hdr.append(f"    {{{n}, {c}, {s[0]}, {s[1]}, {s[2]}, {T}, LinesCfg<{rad_str(s)}, {T}>::THREADS, "
+                       f"LinesCfg<{rad_str(s)}, {T}>::SMEM_BYTES, launch_lines_{n}_{c}}},")
     hdr.append("};")
     hdr.append("static const XPlan kXPlans[] = {")
     for n in x_ns:
-        s = best_split(n)
-        R, _ = x_R(n, s)
-        hdr.append(f"    {{{n}, {s[0]}, {s[1]}, {s[2]}, {R}, XCfg<{rad_str(s)}, {R}>::THREADS, "
-                   f"XCfg<{rad_str(s)}, {R}>::SMEM_BYTES, launch_x_{n}}},")
+        for c, (s, R) in enumerate(x_cands(n)):
+            hdr.append(f"    {{{n}, {c}, {s[0]}, {s[1]}, {s[2]}, {R}, XCfg<{rad_str(s)}, {R}>::THREADS, "
+                       f"XCfg<{rad_str(s)}, {R}>::SMEM_BYTES, launch_x_{n}_{c}}},")
     hdr.append("};")
     hdr.append("static const YPlan kYPlans[] = {")
     for n in y_ns:
-        s_ = best_split(n)
-        hdr.append(f"    {{{n}, {s_[0]}, {s_[1]}, {s_[2]}, YCfg<{rad_str(s_)}>::THREADS, "
-                   f"YCfg<{rad_str(s_)}>::SMEM_BYTES, launch_y_{n}}},")
+        for c, s_ in enumerate(y_cands(n)):
+            hdr.append(f"    {{{n}, {c}, {s_[0]}, {s_[1]}, {s_[2]}, YCfg<{rad_str(s_)}>::THREADS, "
+                       f"YCfg<{rad_str(s_)}>::SMEM_BYTES, launch_y_{n}_{c}}},")
     hdr.append("};")
     hdr.append("}  // namespace dwcu")
     with open(os.path.join(HERE, "plans_gen.h"), "w") as f:
@@ -208,23 +292,34 @@ def main():
                 # the y pass runs faster with scalar complex adds (dft.cuh)
                 lines.append("#define DW_PAIRED_ADDS 0")
             lines += ["#include \"launch.cuh\"", "namespace dwcu {"]
+            if kind == "x":
+                lines += [f"void launch_x_{n}_0(const XArgs &, cudaStream_t);" for n in chunk]
             for n in chunk:
-                s = best_split(n)
                 if kind == "lines":
-                    T, _ = lines_T(n, s)
-                    lines.append(f"void launch_lines_{n}(const LinesArgs &a, int nb, cudaStream_t st) "
-                                 f"{{ launch_lines_t<{rad_str(s)}, {T}>(a, nb, st); }}")
+                    for c, (s, T) in enumerate(lines_cands(n)):
+                        lines.append(f"void launch_lines_{n}_{c}(const LinesArgs &a, int nb, cudaStream_t st) "
+                                     f"{{ launch_lines_t<{rad_str(s)}, {T}>(a, nb, st); }}")
                 elif kind == "x":
-                    R, _ = x_R(n, s)
-                    lines.append(f"void launch_x_{n}(const XArgs &a, cudaStream_t st) "
-                                 f"{{ launch_x_t<{rad_str(s)}, {R}>(a, st); }}")
+                    for c, (s, R) in enumerate(x_cands(n)):
+                        if c == 0:
+                            lines.append(f"void launch_x_{n}_0(const XArgs &a, cudaStream_t st) "
+                                         f"{{ launch_x_t<{rad_str(s)}, {R}>(a, st); }}")
+                        else:
+                            lines.append(f"void launch_x_{n}_{c}(const XArgs &a, cudaStream_t st) "
+                                         f"{{ if (x_iteration_op(a.op)) launch_x_iter_t<{rad_str(s)}, {R}>(a, st); "
+                                         f"else launch_x_{n}_0(a, st); }}")
                 else:
-                    lines.append(f"void launch_y_{n}(const YArgs &a, cudaStream_t st) "
-                                 f"{{ launch_y_t<{rad_str(s)}>(a, st); }}")
+                    for c, s in enumerate(y_cands(n)):
+                        lines.append(f"void launch_y_{n}_{c}(const YArgs &a, cudaStream_t st) "
+                                     f"{{ launch_y_t<{rad_str(s)}>(a, st); }}")
             lines.append("}  // namespace dwcu")
             with open(os.path.join(HERE, f"inst_{kind}_{p}.cu"), "w") as f:
                 f.write("\n".join(lines) + "\n")
-    print(f"lines lengths: {len(lines_ns)}  x half-lengths: {len(x_ns)}  y tiles: {len(y_ns)}")
+    nl = sum(len(lines_cands(n)) for n in lines_ns)
+    nx = sum(len(x_cands(n)) for n in x_ns)
+    ny = sum(len(y_cands(n)) for n in y_ns)
+    print(f"lines lengths: {len(lines_ns)} ({nl} plans)  x half-lengths: {len(x_ns)} ({nx} plans)  "
+          f"y tiles: {len(y_ns)} ({ny} plans)")
 
 
 if __name__ == "__main__":

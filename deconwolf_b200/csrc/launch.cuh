@@ -102,6 +102,23 @@ void launch_x_rows(const XArgs &a, cudaStream_t st)
     }
 }
 
+// the ops of one SHB / RL iteration (ratio + error, update); an alternate
+// radix plan of the autotuner is compiled for these families only
+inline bool x_iteration_op(int op)
+{
+    const int f = x_family(op);
+    return f == XFAM_RATIO || f == XFAM_UPDATE;
+}
+
+template <class RD, int R>
+void launch_x_iter_t(const XArgs &a, cudaStream_t st)
+{
+    if (x_family(a.op) == XFAM_RATIO)
+        launch_x_fam<RD, R, XFAM_RATIO>(a, st);
+    else
+        launch_x_rows<RD, R, XFAM_UPDATE>(a, st);
+}
+
 template <class RD, int R>
 void launch_x_t(const XArgs &a, cudaStream_t st)
 {

@@ -44,7 +44,8 @@ typedef enum dwcu_status {
     DWCU_ERROR_NOT_READY = 6,     /* asynchronous work still running */
     DWCU_ERROR_CANCELLED = 7,     /* a job was cancelled before it finished */
     DWCU_ERROR_TIMEOUT = 8,       /* a bounded wait gave up */
-    DWCU_ERROR_INTERNAL = 9
+    DWCU_ERROR_INTERNAL = 9,
+    DWCU_ERROR_IO = 10            /* a file could not be read or written (tuning tables) */
 } dwcu_status;
 
 /* Enum values equal deconwolf's own (src/dw.h:52-83). */
@@ -280,6 +281,47 @@ int dwcu_fft_c2r(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_ou
  * device is left as it was. */
 int dwcu_fft_r2c_noalloc(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_out, int32_t device,
                          void *stream);
+
+/* ---------------------------------------------------------------- autotuning */
+
+/* The FFT passes have one or more candidate plans per transform length
+ * (radix lists; for the strided line pass also the number of columns per
+ * block); candidate 0 is the generator's heuristic choice.  With tuning on
+ * (the default; DWCU_AUTOTUNE=0 in the environment turns it off), the first
+ * job that needs a length on a device times that length's candidates of
+ * each pass kind on a synthetic volume (CUDA events, a few launches each,
+ * milliseconds in all) and keeps the fastest; later jobs use the recorded
+ * choice.  The first job of a new size therefore takes a little longer to
+ * create, and its creation should not happen during stream capture.
+ * Replaces FFTW's planning by measurement (fft_train, src/fft.c:206-319;
+ * FFTW_MEASURE, src/dw.c:400) and its wisdom files (src/fft.c:236-290):
+ * dwcu_tune_export writes the table as text, dwcu_tune_import reads it back
+ * (imported choices apply to every device and are not measured again). */
+enum { DWCU_TUNE_OFF = 0, DWCU_TUNE_MEASURE = 1 };
+enum { DWCU_PLAN_LINES = 0, DWCU_PLAN_Y = 1, DWCU_PLAN_X = 2 };
+int dwcu_tune_set_mode(int32_t mode);
+int dwcu_tune_get_mode(int32_t *mode);
+/* The selection rule, on candidate times in ms: the index of the fastest,
+ * unless it is not faster than candidate 0 by more than `margin` (relative),
+ * in which case 0.  Non-finite or negative times are candidates that could
+ * not run.  (Pure host logic.) */
+int dwcu_tune_select(const float *ms, int32_t n, float margin, int32_t *choice);
+/* Candidates of a length for a pass kind (0: length not supported). */
+int dwcu_tune_plan_count(int32_t kind, int32_t n, int32_t *count);
+/* Radix list (radices[3], 1 = unused) and tile of one candidate: columns per
+ * block (lines), rows per block (x), lines per tile (y, always 4). */
+int dwcu_tune_plan_info(int32_t kind, int32_t n, int32_t cand, int32_t *radices, int32_t *tile);
+/* Use candidate `cand` for this length on every device from now on (cand -1:
+ * forget the length, so the next job measures it again). */
+int dwcu_tune_force(int32_t kind, int32_t n, int32_t cand);
+/* Time the candidates of one length on a device now (if not recorded yet). */
+int dwcu_tune_run(int32_t device, int32_t kind, int32_t n);
+/* The recorded choice for (device, kind, n): *cand = -1 if none; ms[i] the
+ * measured time of candidate i (*nms of them; 0 when imported or forced). */
+int dwcu_tune_query(int32_t device, int32_t kind, int32_t n, int32_t *cand, float *ms, int32_t cap, int32_t *nms);
+int dwcu_tune_clear(void);
+int dwcu_tune_export(const char *path);
+int dwcu_tune_import(const char *path);
 
 /* ---------------------------------------------------------------- timing */
 
