@@ -320,6 +320,75 @@ def run_channels(args):
     return 0
 
 
+# jobs per size class of the serving stream (a few seconds of GPU work each)
+CLASS_JOBS = (24, 12, 4, 2)
+
+
+def run_classes(args):
+    """Plain vs batched per size class of the serving stream: for each image
+    size, CLASS_JOBS jobs of 50 SHB iterations (two seeded images of the
+    class alternating, the 525 nm PSF of the class), run one at a time through
+    dwcu_deconvolve and as one dwcu_batch_run; page-locked host buffers,
+    uploads and downloads inside the timed region, wall clock."""
+    import deconwolf_b200 as dw
+    from deconwolf_b200 import synthetic
+    classes = []
+    for size, njobs in enumerate(CLASS_JOBS):
+        if args.classes and size not in args.classes:
+            continue
+        ims = [_pinned(synthetic.serve_image(size, v, CACHE)[0]) for v in range(2)]
+        psf = dw.psf_prepare(synthetic.serve_psf(size, 525.0, CACHE), ims[0].shape)
+        jobs_in = [ims[i % 2] for i in range(njobs)]
+        outs_b = [_pinned(shape=ims[0].shape) for _ in range(njobs)]
+        outs_s = [_pinned(shape=ims[0].shape) for _ in range(njobs)]
+
+        def batched():
+            jobs = []
+            for im in jobs_in:
+                j = dw.Job(im.shape, psf.shape, method="shb", n_iter=ITERS)
+                j.setup(im, psf)
+                jobs.append(j)
+            dw.batch_run(jobs)
+            res = [j.result(out=o) for j, o in zip(jobs, outs_b)]
+            for j in jobs:
+                j.close()
+            return res
+
+        def sequential():
+            return [dw.run_method(im, psf, out=o, method="shb", n_iter=ITERS) for im, o in zip(jobs_in, outs_s)]
+
+        for _ in range(args.warmup):
+            batched()
+            sequential()
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            rb = batched()
+        dt_b = (time.perf_counter() - t) / args.steps
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            rs = sequential()
+        dt_s = (time.perf_counter() - t) / args.steps
+        vox_it = float(ims[0].size) * ITERS * njobs
+        work = dw.plan_size(ims[0].shape, psf.shape)[0]
+        same = all(np.array_equal(a.out, b.out) for a, b in zip(rb, rs))
+        classes.append({"image": list(ims[0].shape[::-1]), "job": list(work), "psf": list(psf.shape[::-1]),
+                        "jobs": njobs, "batched": vox_it / dt_b / 1e6, "sequential": vox_it / dt_s / 1e6,
+                        "ratio": dt_s / dt_b, "batched_ms": dt_b * 1e3, "sequential_ms": dt_s * 1e3,
+                        "batched_equals_sequential": bool(same)})
+        log(f"class {size}: {classes[-1]}")
+    tot_b = sum(c["batched_ms"] for c in classes)
+    tot_s = sum(c["sequential_ms"] for c in classes)
+    vox = sum(c["batched"] * c["batched_ms"] for c in classes)
+    print(json.dumps(_common_line(
+        "Mvoxel*iter/s (SHB 50 it, batches of one size class)", vox / tot_b, args,
+        {"workload": "batch-classes", "method": "shb", "iterations": ITERS,
+         "host_buffers": "page-locked images and results"},
+        {"ms_per_step": tot_b, "classes": classes,
+         "sequential": {"value": vox / tot_s, "ms_per_step": tot_s,
+                        "how": "dwcu_deconvolve per job, one after another"}})), flush=True)
+    return 0
+
+
 def run_serve(args):
     import deconwolf_b200 as dw
     from deconwolf_b200 import synthetic
@@ -400,10 +469,12 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=[WORKLOAD, SMALL, PROFILE_CASE, "shb-2048x256x20", "shb-256x2048x20", "shb-256x256x60",
                              "shb-1124x1124x60",
-                             "tiles-4096x4096x60", "channels-6", "serve-stream"])
+                             "tiles-4096x4096x60", "channels-6", "serve-stream", "batch-classes"])
     ap.add_argument("--tilesize", type=int, default=1024)
     ap.add_argument("--requests", type=int, default=60, help="serve-stream: number of requests (full stream: 500)")
     ap.add_argument("--hbm-budget", type=float, default=160e9, help="serve-stream: device bytes for admitted jobs")
+    ap.add_argument("--classes", type=int, nargs="*", default=None,
+                    help="batch-classes: size classes to run (default: all four)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -418,6 +489,8 @@ def main():
         return run_channels(args)
     if args.workload == "serve-stream":
         return run_serve(args)
+    if args.workload == "batch-classes":
+        return run_classes(args)
 
     import torch
     import torch.distributed as dist

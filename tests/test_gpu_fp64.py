@@ -24,7 +24,7 @@ from tests.helpers import gauss_psf, poisson_image, rel_l2, sketch, sketch_rel_l
 
 pytestmark = pytest.mark.gpu
 
-FP64_FACTOR = 8.0
+FP64_FACTOR = 4.0
 FP64_FLOOR = 1e-6
 
 
