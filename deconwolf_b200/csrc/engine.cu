@@ -379,7 +379,7 @@ static std::mutex g_blk_mu;
 static std::map<int, std::vector<Block *>> g_blk_free;
 // released blocks kept per device: at most this many, and at most half of
 // the device's memory together
-constexpr size_t kMaxCachedBlocks = 8;
+constexpr size_t kMaxCachedBlocks = 64;
 
 static size_t device_total_bytes(int device)
 {
@@ -1499,19 +1499,14 @@ static int batch_run(dwcu_job **jobs, int n, cudaStream_t origin)
         cudaEventDestroy(e);
     }
     if (!fixed_idx.empty()) {
-        bool prof;
-        {
-            std::lock_guard<std::mutex> lk(g_prof_mu);
-            prof = g_prof_on;
-        }
-        const bool graph = !prof;
-        cudaGraph_t gr = nullptr;
-        if (graph) CU(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal));
+        // Each job's remaining loop is one CUDA graph, cached on its memory
+        // block (captured the first time a job of these sizes and options
+        // runs on that block, replayed after that), launched on the job's own
+        // stream, so small jobs run side by side.  Jobs that fill the GPU on
+        // their own run one after another on one stream: side by side they
+        // would only compete for the SMs and evict each other's data from L2
+        // between passes.
         cudaEventRecord(fork, origin);
-        // Jobs that fill the GPU on their own run one after another on one
-        // chain: side by side they would only compete for the SMs and evict
-        // each other's data from L2 between passes.  Smaller jobs run as
-        // chains of their own beside them.
         int big_chain = -1;
         for (int i : fixed_idx) {
             dwcu_job *j = jobs[i];
@@ -1523,30 +1518,9 @@ static int batch_run(dwcu_job **jobs, int n, cudaStream_t origin)
                     j->stream = streams[(size_t) big_chain];
             }
             cudaStreamWaitEvent(j->stream, fork, 0);
-            const int ug = j->s.use_graph;
-            j->s.use_graph = 0;  // eager launches: captured into the batch graph
             if (rc == DWCU_SUCCESS) rc = job_step_impl(j, 1 << 30, nullptr);
-            j->s.use_graph = ug;
             cudaEventRecord(done, j->stream);
             cudaStreamWaitEvent(origin, done, 0);
-        }
-        if (graph) {
-            cudaError_t ce = cudaStreamEndCapture(origin, &gr);
-            if (rc == DWCU_SUCCESS && ce != cudaSuccess)
-                rc = fail(DWCU_ERROR_CUDA, "batch capture failed: %s", cudaGetErrorString(ce));
-            cudaGraphExec_t ex = nullptr;
-            if (rc == DWCU_SUCCESS) {
-                ce = cudaGraphInstantiate(&ex, gr, 0);
-                if (ce != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "batch instantiate failed: %s", cudaGetErrorString(ce));
-            }
-            if (gr) cudaGraphDestroy(gr);
-            if (rc == DWCU_SUCCESS) {
-                if (cudaGraphLaunch(ex, origin) != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "batch launch failed");
-            }
-            if (ex) {
-                cudaStreamSynchronize(origin);
-                cudaGraphExecDestroy(ex);
-            }
         }
     }
     // stopping rules that read the error back: round-robin, one iteration at a time

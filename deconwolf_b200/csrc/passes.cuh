@@ -43,10 +43,15 @@ struct Rad {
     static constexpr bool THREE = (RC > 1);
     static constexpr int RL = THREE ? RC : RB;  // last radix
     static constexpr int TPL = cmax(cmax(N / RA, N / RB), THREE ? N / RC : 0);
-    // padded exchange index: one spare slot per RA block keeps the
-    // stride-RA writes of the first stage free of bank conflicts
+    // padded exchange index: for an even first radix, one spare slot per RA
+    // block makes the first stage's stride-RA writes an odd number of
+    // float2 apart, which keeps them free of bank conflicts; an odd RA
+    // already is, and a spare slot would make the stride even (for RA = 15,
+    // every thread of a warp on the same bank), so odd RA is not padded.
+    // PADN (the tile size) is the padded bound either way.
+    static constexpr int PK = (RA % 2 == 0) ? 1 : 0;
     static constexpr int PADN = N + N / RA + 1;
-    static __device__ __forceinline__ int pad(int idx) { return idx + idx / RA; }
+    static __device__ __forceinline__ int pad(int idx) { return idx + PK * (idx / RA); }
 };
 
 // Twiddles of one Stockham stage for butterfly index j: W^r with
@@ -128,11 +133,11 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
 {
     constexpr int N = RD::N, RA = RD::RA, RB = RD::RB, RC = RD::RC;
     constexpr int M2 = N / RB;  // stage-2 butterflies; read stride, a multiple of RA
-    // stage 1 writes t*RA + r  ->  padded t*(RA+1) + r
+    // stage 1 writes t*RA + r  ->  padded t*(RA+PK) + r
     if (t < N / RA) {
         float2 none[RA];
         butterfly<1, RA, DIR, Q>(v, none);
-        const int b1 = t * (RA + 1);
+        const int b1 = t * (RA + RD::PK);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
 #pragma unroll
@@ -149,7 +154,7 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
-                for (int r = 0; r < RB; ++r) u[q][r] = *smem(q, b2 + r * (M2 + M2 / RA));
+                for (int r = 0; r < RB; ++r) u[q][r] = *smem(q, b2 + r * (M2 + RD::PK * (M2 / RA)));
         }
         if constexpr (!PP) __syncthreads();
         if (t < M2) {
@@ -157,11 +162,11 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
             else if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
             butterfly<RA, RB, DIR, Q>(u, w2);
             const int base = (t / RA) * RA * RB + t % RA;  // writes base + r*RA
-            const int b3 = base + base / RA;
+            const int b3 = base + RD::PK * (base / RA);
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
-                for (int r = 0; r < RB; ++r) *smem2(q, b3 + r * (RA + 1)) = u[q][r];
+                for (int r = 0; r < RB; ++r) *smem2(q, b3 + r * (RA + RD::PK)) = u[q][r];
         }
         float2 w3[RC];
         if (PREF && t < M3) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
@@ -171,7 +176,7 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
-                for (int r = 0; r < RC; ++r) o[q][r] = *smem2(q, b4 + r * (M3 + M3 / RA));
+                for (int r = 0; r < RC; ++r) o[q][r] = *smem2(q, b4 + r * (M3 + RD::PK * (M3 / RA)));
             if constexpr (HOIST) stage_twiddles_from<RC>(w3, tb3);
             else if (!PREF) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
             butterfly<RA * RB, RC, DIR, Q>(o, w3);
@@ -182,7 +187,7 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
-                for (int r = 0; r < RB; ++r) o[q][r] = *smem(q, b2 + r * (M2 + M2 / RA));
+                for (int r = 0; r < RB; ++r) o[q][r] = *smem(q, b2 + r * (M2 + RD::PK * (M2 / RA)));
             if constexpr (HOIST) stage_twiddles_from<RB>(w2, tb2);
             else if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
             butterfly<RA, RB, DIR, Q>(o, w2);

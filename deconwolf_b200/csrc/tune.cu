@@ -8,7 +8,7 @@
 // is the analogue of deconwolf's FFTW planning by measurement (fft_train,
 // src/fft.c:206-319, FFTW_MEASURE by default, src/dw.c:400) and of its
 // wisdom files (fftwf_import/export_wisdom_from/to_filename, src/fft.c:
-// 236-290): the table can be written to a text file and read back, so a
+// 299-316 and 355): the table can be written to a text file and read back, so a
 // later process skips the measurements.
 //
 // Selection: the fastest candidate wins only if it beats candidate 0 by

@@ -132,11 +132,13 @@ int dwcu_job_setup(dwcu_job *job, const float *im, const float *psf, int32_t on_
  * s->iter_type is applied; REL and ABS read each error back (one small copy
  * per iteration).  *remaining receives how many iterations may still run. */
 int dwcu_job_step(dwcu_job *job, int32_t n, int32_t *remaining);
-/* Run set-up jobs to completion together: jobs with a fixed iteration count
- * become chains of one CUDA graph: jobs large enough to fill the GPU
- * (>= 32 Mi padded voxels) one after another on one chain, smaller ones on
- * chains of their own beside them, so tiles and channels of uneven sizes
- * share the GPU; REL/ABS jobs are stepped round-robin.  Replaces the sequential tile loop of deconvolve_tiles
+/* Run set-up jobs to completion together: each job with a fixed iteration
+ * count replays its iteration loop as one CUDA graph (cached with its
+ * device block, so a job of the same sizes on a reused block captures
+ * nothing) on a stream of its own; jobs large enough to fill the GPU
+ * (>= 32 Mi padded voxels) run one after another on one stream, smaller
+ * ones side by side, so tiles and channels of uneven sizes share the GPU;
+ * REL/ABS jobs are stepped round-robin.  Replaces the sequential tile loop of deconvolve_tiles
  * (src/dw.c:2093-2153) for the iteration part.  Returns when all are done;
  * results are then read with dwcu_job_result. */
 int dwcu_batch_run(dwcu_job **jobs, int32_t n, void *stream);
@@ -146,7 +148,7 @@ int dwcu_job_done(const dwcu_job *job);
  * and the error trace.  Fills s-like outputs into *s_out when non-NULL. */
 int dwcu_job_result(dwcu_job *job, float *out, int32_t out_on_device, dwcu_opts *s_out);
 /* Release the job.  Its device block is kept by the library for the next
- * job of a similar size (at most eight blocks and half of the device's
+ * job of a similar size (at most 64 blocks and half of the device's
  * memory per device); dwcu_release_cache frees those. */
 void dwcu_job_destroy(dwcu_job *job);
 /* Free the device blocks the library keeps for reuse on `device` (all
@@ -294,7 +296,7 @@ int dwcu_fft_r2c_noalloc(const float *d_in, int64_t M, int64_t N, int64_t P, flo
  * choice.  The first job of a new size therefore takes a little longer to
  * create, and its creation should not happen during stream capture.
  * Replaces FFTW's planning by measurement (fft_train, src/fft.c:206-319;
- * FFTW_MEASURE, src/dw.c:400) and its wisdom files (src/fft.c:236-290):
+ * FFTW_MEASURE, src/dw.c:400) and its wisdom files (src/fft.c:299-316, 355):
  * dwcu_tune_export writes the table as text, dwcu_tune_import reads it back
  * (imported choices apply to every device and are not measured again). */
 enum { DWCU_TUNE_OFF = 0, DWCU_TUNE_MEASURE = 1 };

@@ -107,6 +107,33 @@ def available(kind: str) -> bool:
     return os.path.exists(PORT_SO if kind == "port" else REF_SO)
 
 
+PSF_SO = os.path.join(HERE, "_ref", "libdwpsf.so")
+
+
+def psf_prepare_reference(psf: np.ndarray, shape, border_quality: int = 2, xycropfactor: float = 0.001):
+    """deconwolf's own PSF preparation (dw_run, src/dw.c:2799-2826: normalise,
+    psf_autocrop, normalise), from _ref/libdwpsf.so (dw.c compiled
+    unmodified); None when that build is absent."""
+    if not os.path.exists(PSF_SO):
+        return None
+    lib = _libs.get("psf")
+    if lib is None:
+        lib = ctypes.CDLL(PSF_SO)
+        lib.dwpsf_prepare.restype = ctypes.c_int
+        lib.dwpsf_prepare.argtypes = [ctypes.c_void_p] + [ctypes.c_int64] * 6 + [ctypes.c_int, ctypes.c_float,
+                                                                                  ctypes.c_void_p, ctypes.c_void_p]
+        _libs["psf"] = lib
+    p = np.ascontiguousarray(psf, dtype=np.float32)
+    P, N, M = shape
+    pP, pN, pM = p.shape
+    out = np.empty(p.size, dtype=np.float32)
+    dims = (ctypes.c_int64 * 3)()
+    rc = lib.dwpsf_prepare(p.ctypes.data, pM, pN, pP, M, N, P, border_quality, xycropfactor, out.ctypes.data, dims)
+    if rc != 0:
+        raise RuntimeError("dwpsf_prepare failed")
+    return out[: dims[0] * dims[1] * dims[2]].reshape(dims[2], dims[1], dims[0]).copy()
+
+
 class Result:
     def __init__(self, out, trace, opts: DwoOpts):
         self.out = out

@@ -107,6 +107,28 @@ PSF_CASES = [
 
 
 @pytest.mark.parametrize("pshape,ishape,bq,xy", PSF_CASES)
+def test_psf_prepare_equals_reference(pshape, ishape, bq, xy):
+    """dwcu_psf_prepare against deconwolf's own dw.c (psf_autocrop compiled
+    unmodified into oracle/_ref/libdwpsf.so), bit for bit."""
+    psf = gauss_psf(pshape, (pshape[0] / 6, pshape[1] / 8, pshape[2] / 7), seed=2, jitter=0.1)
+    ref = po.psf_prepare_reference(psf, ishape, bq, xy)
+    if ref is None:
+        pytest.skip("reference PSF preparation not built (needs deconwolf's sources)")
+    np.testing.assert_array_equal(dw.psf_prepare(psf, ishape, bq, xy), ref)
+
+
+def test_psf_prepare_born_wolf_equals_reference():
+    """The Born-Wolf PSFs of the benchmark workloads, prepared for their images."""
+    from deconwolf_b200 import synthetic
+    for pshape, ishape, lam in (((79, 127, 127), (40, 256, 256), 466.0), ((39, 121, 121), (20, 256, 256), 525.0)):
+        psf = synthetic.bw_psf(pshape, lam=lam)
+        ref = po.psf_prepare_reference(psf, ishape, 2, 0.001)
+        if ref is None:
+            pytest.skip("reference PSF preparation not built (needs deconwolf's sources)")
+        np.testing.assert_array_equal(dw.psf_prepare(psf, ishape, 2, 0.001), ref)
+
+
+@pytest.mark.parametrize("pshape,ishape,bq,xy", PSF_CASES)
 def test_psf_prepare_equals_oracle(pshape, ishape, bq, xy):
     psf = gauss_psf(pshape, (pshape[0] / 6, pshape[1] / 8, pshape[2] / 7), seed=2, jitter=0.1)
     a = dw.psf_prepare(psf, ishape, bq, xy)

@@ -1,6 +1,6 @@
 """The autotuner's host logic (CPU): the selection rule on given candidate
 times, the candidate table, and the plan-table file round trip (the
-analogue of FFTW wisdom files, src/fft.c:236-290)."""
+analogue of FFTW wisdom files, src/fft.c:299-316, 355)."""
 import math
 
 import pytest
