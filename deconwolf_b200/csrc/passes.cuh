@@ -114,23 +114,28 @@ __device__ __forceinline__ void butterfly(float2 (&v)[Q][R], const float2 (&w)[R
 // barrier is needed between its reads and its writes; stage 3 reads smem2.
 // HOIST: the stage twiddles come from tb2 / tb3 (stage_twiddle_base of
 // stages 2 and 3 for this thread, kept by the caller) instead of the table
-template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2, bool HOIST = false>
+// PAD2: the second exchange (stage-2 writes in runs of RA, stage-3
+// unit-stride reads) is padded like the first; without it its reads are
+// conflict-free.  Measured: unpadded is faster for the x pass (one line per
+// thread row), padded for the y pass (four lines interleaved).
+template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2, bool HOIST = false, bool PAD2 = true>
 __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
                                               const float2 *__restrict__ tw, SM smem, SM2 smem2,
                                               float2 tb2 = float2{}, float2 tb3 = float2{});
 
-template <class RD, int DIR, int Q, bool PREF = false, class SM>
+template <class RD, int DIR, int Q, bool PREF = false, bool PAD2 = true, class SM>
 __device__ __forceinline__ void line_fft(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
                                          const float2 *__restrict__ tw, SM smem)
 {
-    line_fft_impl<RD, DIR, Q, PREF, false>(v, o, t, tw, smem, smem);
+    line_fft_impl<RD, DIR, Q, PREF, false, SM, SM, false, PAD2>(v, o, t, tw, smem, smem);
 }
 
-template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2, bool HOIST>
+template <class RD, int DIR, int Q, bool PREF, bool PP, class SM, class SM2, bool HOIST, bool PAD2>
 __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o)[Q][RD::RL], int t,
                                               const float2 *__restrict__ tw, SM smem, SM2 smem2, float2 tb2,
                                               float2 tb3)
 {
+    constexpr int P2 = PAD2 ? RD::PK : 0;  // padding of the second exchange
     constexpr int N = RD::N, RA = RD::RA, RB = RD::RB, RC = RD::RC;
     constexpr int M2 = N / RB;  // stage-2 butterflies; read stride, a multiple of RA
     // stage 1 writes t*RA + r  ->  padded t*(RA+PK) + r
@@ -162,21 +167,21 @@ __device__ __forceinline__ void line_fft_impl(float2 (&v)[Q][RD::RA], float2 (&o
             else if (!PREF) stage_twiddles<N, RA, RB>(w2, t, tw);
             butterfly<RA, RB, DIR, Q>(u, w2);
             const int base = (t / RA) * RA * RB + t % RA;  // writes base + r*RA
-            const int b3 = base + RD::PK * (base / RA);
+            const int b3 = base + P2 * (base / RA);
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
-                for (int r = 0; r < RB; ++r) *smem2(q, b3 + r * (RA + RD::PK)) = u[q][r];
+                for (int r = 0; r < RB; ++r) *smem2(q, b3 + r * (RA + P2)) = u[q][r];
         }
         float2 w3[RC];
         if (PREF && t < M3) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
         __syncthreads();
         if (t < M3) {
-            const int b4 = RD::pad(t);
+            const int b4 = t + P2 * (t / RA);
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
-                for (int r = 0; r < RC; ++r) o[q][r] = *smem2(q, b4 + r * (M3 + RD::PK * (M3 / RA)));
+                for (int r = 0; r < RC; ++r) o[q][r] = *smem2(q, b4 + r * (M3 + P2 * (M3 / RA)));
             if constexpr (HOIST) stage_twiddles_from<RC>(w3, tb3);
             else if (!PREF) stage_twiddles<N, RA * RB, RC>(w3, t, tw);
             butterfly<RA * RB, RC, DIR, Q>(o, w3);
@@ -878,7 +883,7 @@ k_xpass(XArgs a)
             });
         }
         __syncthreads();  // the staged rows become the exchange tiles
-        line_fft<RD, +1, Q, PREF_TW>(v, w, t, a.twL, smem);
+        line_fft<RD, +1, Q, PREF_TW, false>(v, w, t, a.twL, smem);
     }
     if (!wait_all(&bars[1], 0, a.err, 3 << 8)) return;
 
@@ -958,7 +963,8 @@ k_xpass(XArgs a)
     // the barrier after stage 1), so stage 3 leaves the exchange tiles free
     float2 *xb2 = reinterpret_cast<float2 *>(RB);
     auto smem2 = [&](int q, int i) { return xb2 + (size_t) (ry * Q + q) * C::ROW_F2 + i; };
-    line_fft_impl<RV, -1, Q, PREF_TW, true>(w, qo, t, a.twL, smem, smem2);
+    line_fft_impl<RV, -1, Q, PREF_TW, true, decltype(smem), decltype(smem2), false, false>(w, qo, t, a.twL, smem,
+                                                                                           smem2);
     constexpr int SQ = L / RV::RL;
     if constexpr (!RV::THREE) __syncthreads();
     if (t < SQ) {
