@@ -18,9 +18,11 @@ the FP64 result at the same sampled voxels, its trace, norm and sketch
 (tests/helpers.sketch), the reference output's sketch and the reference's
 exact relative L2 distance to the FP64 result.
 
---config2 (about 40 minutes on 8 cores, ~35 GB of RAM) runs the reference's
+--config2 (one to two hours on 8 cores, ~20 GB of RAM) runs the reference's
 SHB for 50 iterations on the 2048 x 2048 x 60 workload and stores its trace,
 plane sums, norm, 262144 sampled voxels and a sketch of the whole output.
+--tile1024 does the same for one interior tile of the tiled 4096 x 4096 x 60
+workload (1124 x 1124 x 60 with the full PSF).
 """
 from __future__ import annotations
 
@@ -116,11 +118,34 @@ def config2():
         bg=np.float32(r.bg), loop_seconds=np.float64(r.loop_seconds), threads=np.int64(os.cpu_count()))
 
 
+def tile1024():
+    """One interior tile of the 4096 x 4096 x 60 image at tile size 1024 and
+    overlap 50 (1124 x 1124 x 60), with the full 181 x 181 x 119 PSF: the
+    transform lengths of the tiled workload (job 1304 x 1304 x 178, padded on
+    the GPU to 1344 x 1344 x 180), SHB 50 iterations."""
+    from deconwolf_b200 import synthetic
+    from tests.helpers import sketch
+    name = "shb-1124x1124x60"
+    im, psf = synthetic.config_inputs(name)
+    t = time.time()
+    r = po.deconvolve(im, psf, method="shb", n_iter=50, impl="reference", threads=os.cpu_count())
+    print("reference SHB 1124x1124x60, 50 it:", time.time() - t, "s", flush=True)
+    idx = np.sort(sample_index(im.shape, 131072))
+    out = r.out
+    np.savez_compressed(
+        os.path.join(HERE, "tile1024_shb50.npz"),
+        trace=r.trace, plane_sums=out.astype(np.float64).sum(axis=(1, 2)), sample_idx=idx,
+        sample_val=out.reshape(-1)[idx], norm=np.float64(np.linalg.norm(out.astype(np.float64))),
+        sketch=sketch(out), image_sum=np.float64(im.astype(np.float64).sum()), image_sample=im.reshape(-1)[idx],
+        bg=np.float32(r.bg), loop_seconds=np.float64(r.loop_seconds), threads=np.int64(os.cpu_count()))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--config1", action="store_true")
     ap.add_argument("--config1-fp64", action="store_true")
     ap.add_argument("--config2", action="store_true")
+    ap.add_argument("--tile1024", action="store_true")
     ap.add_argument("--no-small", action="store_true")
     a = ap.parse_args()
     if not a.no_small:
@@ -134,6 +159,8 @@ def main():
         config1_fp64()
     if a.config2:
         config2()
+    if a.tile1024:
+        tile1024()
 
 
 if __name__ == "__main__":
