@@ -128,7 +128,7 @@ EXPORTS = [
     "dwcu_server_destroy", "dwcu_tile_blend", "dwcu_release_cache",
     "dwcu_tune_set_mode", "dwcu_tune_get_mode", "dwcu_tune_select", "dwcu_tune_plan_count",
     "dwcu_tune_plan_info", "dwcu_tune_force", "dwcu_tune_run", "dwcu_tune_query", "dwcu_tune_clear",
-    "dwcu_tune_export", "dwcu_tune_import",
+    "dwcu_tune_export", "dwcu_tune_import", "dwcu_psf_prepare_device",
 ]
 
 # pass kinds of the autotuner (dwcu.h)
@@ -218,6 +218,9 @@ def lib() -> ctypes.CDLL:
                L.dwcu_tune_plan_info, L.dwcu_tune_force, L.dwcu_tune_run, L.dwcu_tune_query, L.dwcu_tune_clear,
                L.dwcu_tune_export, L.dwcu_tune_import):
         fn.restype = ctypes.c_int
+    L.dwcu_psf_prepare_device.argtypes = [vp, i64, i64, i64, i64, i64, i64, i32, ctypes.c_float, vp,
+                                          ctypes.POINTER(i64), i32, vp]
+    L.dwcu_psf_prepare_device.restype = ctypes.c_int
     L.dwcu_batch_run.argtypes = [ctypes.POINTER(vp), i32, vp]
     L.dwcu_batch_run.restype = ctypes.c_int
     L.dwcu_psf_prepare.argtypes = [vp, i64, i64, i64, i64, i64, i64, i32, ctypes.c_float, vp,
@@ -372,6 +375,18 @@ def psf_prepare(psf: np.ndarray, shape, border_quality: int = 2, xycropfactor: f
     _check(lib().dwcu_psf_prepare(p.ctypes.data, pM, pN, pP, M, N, P, border_quality, xycropfactor,
                                   out.ctypes.data, dims))
     return out[: dims[0] * dims[1] * dims[2]].reshape(dims[2], dims[1], dims[0]).copy()
+
+
+def psf_prepare_device(d_psf: int, psf_shape, shape, d_out: int, border_quality: int = 2,
+                       xycropfactor: float = 0.001, device: int = 0, stream: int = 0):
+    """:func:`psf_prepare` on device buffers (d_psf, d_out: device pointers,
+    d_out with room for the whole PSF); returns the prepared (P, N, M) size."""
+    P, N, M = shape
+    pP, pN, pM = psf_shape
+    dims = (ctypes.c_int64 * 3)()
+    _check(lib().dwcu_psf_prepare_device(ctypes.c_void_p(d_psf), pM, pN, pP, M, N, P, border_quality, xycropfactor,
+                                         ctypes.c_void_p(d_out), dims, device, ctypes.c_void_p(stream or None)))
+    return (int(dims[2]), int(dims[1]), int(dims[0]))
 
 
 def tiling_create(shape, max_size: int, overlap: int = 20) -> list[dict]:

@@ -124,6 +124,165 @@ static void crop_xy(std::vector<float> &psf, int64_t &pM, int64_t &pN, int64_t p
     pN -= 2 * first;
 }
 
+// ------------------------------------------------------------ PSF preparation on the device
+//
+// The same steps as above on a device copy of the PSF, for the GPU's own
+// set-up (the tiled path): the double sums of the normalisations as a
+// fixed-order tree (a fixed grid of partial sums, then one thread), each
+// value divided in double and rounded to float as fim_normalize_sum1 does
+// (fim.c:900-912; the reference's own sum is an OpenMP reduction, so its
+// order varies with the thread count, which moves the double sum by
+// rounding only); the x-plane sums of psf_autocrop_XY in float, one thread
+// per plane in the reference's order (y outer, z inner, dw.c:1885-1907), so
+// the crop decision is the reference's bit for bit.
+
+constexpr int kPsfSumBlocks = 128;
+constexpr int kPsfThreads = 256;
+
+__global__ void k_psf_sum_partial(const float *__restrict__ p, long long n, double *__restrict__ part)
+{
+    __shared__ double sh[kPsfThreads];
+    double s = 0;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x)
+        s += (double) p[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = kPsfThreads / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_psf_sum_final(const double *__restrict__ part, int n, double *__restrict__ out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0;
+        for (int i = 0; i < n; ++i) s += part[i];
+        *out = s;
+    }
+}
+
+// out = the cuboid [m0, m0+m) x [n0, n0+n) x [p0, p0+p) of in (M x N x ...),
+// divided by *sum when sum is given (fim_get_cuboid, fim.c:659-693)
+__global__ void k_psf_crop_scale(const float *__restrict__ in, long long M, long long N, long long m0, long long n0,
+                                 long long p0, long long m, long long n, long long p, const double *__restrict__ sum,
+                                 float *__restrict__ out)
+{
+    const long long tot = m * n * p;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < tot; i += (long long) gridDim.x * blockDim.x) {
+        const long long a = i % m, b = (i / m) % n, c = i / (m * n);
+        const float v = in[(a + m0) + (b + n0) * M + (c + p0) * M * N];
+        out[i] = sum ? (float) ((double) v / *sum) : v;
+    }
+}
+
+// psf_autocrop_XY's decision (dw.c:1862-1912): the float sum of every x
+// plane in the reference's order, the largest of them, and the first plane
+// whose sum reaches xycropfactor times it
+__global__ void k_psf_plane_sums(const float *__restrict__ p, long long M, long long N, long long P,
+                                 float *__restrict__ plane)
+{
+    const long long xx = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if (xx >= M) return;
+    float sum = 0.f;
+    for (long long yy = 0; yy < N; ++yy)
+        for (long long zz = 0; zz < P; ++zz) sum += p[xx + yy * M + zz * M * N];
+    plane[xx] = sum;
+}
+
+__global__ void k_psf_first_plane(const float *__restrict__ plane, long long M, float factor, long long *first_out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    float maxsum = 0.f;
+    for (long long xx = 0; xx < M; ++xx)
+        if (plane[xx] > maxsum) maxsum = plane[xx];
+    long long first = -1;
+    float sum = 0.f;
+    while (sum < factor * maxsum && first + 1 < M) {
+        first++;
+        sum = plane[first];
+    }
+    *first_out = first;
+}
+
+// d_out (room for pM*pN*pP floats) receives the prepared PSF; dims[3] its
+// size.  Scratch is allocated here and freed before returning; the call
+// waits for its stream (the caller needs the size).
+static int psf_prepare_device(const float *d_psf, int64_t pM, int64_t pN, int64_t pP, int64_t M, int64_t N,
+                              int64_t P, int bq, float xycropfactor, float *d_out, int64_t dims[3], cudaStream_t st)
+{
+    const long long n0 = pM * pN * pP;
+    char *scratch = nullptr;
+    // partials, two sums, the first plane, the x-plane sums, two cuboids
+    const size_t o_part = 0, o_sum = 1024 + 8 * kPsfSumBlocks, o_first = o_sum + 256, o_plane = o_first + 256;
+    const size_t o_b1 = o_plane + ((size_t) (4 * pM) + 255) / 256 * 256;
+    const size_t o_b2 = o_b1 + ((size_t) (4 * n0) + 255) / 256 * 256;
+    const size_t bytes = o_b2 + ((size_t) (4 * n0) + 255) / 256 * 256;
+    HCU(cudaMalloc(&scratch, bytes));
+    struct Free {
+        char *p;
+        ~Free() { cudaFree(p); }
+    } guard{scratch};
+    double *part = (double *) (scratch + o_part), *sum1 = (double *) (scratch + o_sum), *sum2 = sum1 + 1;
+    long long *first_d = (long long *) (scratch + o_first);
+    float *plane = (float *) (scratch + o_plane), *b1 = (float *) (scratch + o_b1), *b2 = (float *) (scratch + o_b2);
+    auto dsum = [&](const float *p, long long n, double *out) -> int {
+        k_psf_sum_partial<<<kPsfSumBlocks, kPsfThreads, 0, st>>>(p, n, part);
+        k_psf_sum_final<<<1, 32, 0, st>>>(part, kPsfSumBlocks, out);
+        dwcu::record_launch();
+        dwcu::record_launch();
+        return cudaGetLastError() == cudaSuccess ? DWCU_SUCCESS : fail(DWCU_ERROR_CUDA, "PSF sum launch failed");
+    };
+    auto crop = [&](const float *in, long long Mi, long long Ni, long long m0, long long nn0, long long p0,
+                    long long m, long long n, long long p, const double *sc, float *out) -> int {
+        const long long tot = m * n * p;
+        const int blocks = (int) std::min<long long>(148 * 8, (tot + kPsfThreads - 1) / kPsfThreads);
+        k_psf_crop_scale<<<std::max(blocks, 1), kPsfThreads, 0, st>>>(in, Mi, Ni, m0, nn0, p0, m, n, p, sc, out);
+        dwcu::record_launch();
+        return cudaGetLastError() == cudaSuccess ? DWCU_SUCCESS : fail(DWCU_ERROR_CUDA, "PSF crop launch failed");
+    };
+    // normalise (dw.c:2799), crop against the image (psf_autocrop_byImage)
+    int rc = dsum(d_psf, n0, sum1);
+    int64_t a0 = 0, a1 = pM - 1, c0 = 0, c1 = pN - 1, e0 = 0, e1 = pP - 1;
+    {
+        int64_t mopt = (M - 1) * 2 + 1, nopt = (N - 1) * 2 + 1, popt = (P - 1) * 2 + 1;
+        if (bq == 0) { mopt = M; nopt = N; popt = P; }
+        if (pP >= popt && (pM > mopt || pN > nopt || pP > popt)) {
+            if (pM > mopt) { a0 = (pM - mopt) / 2; a1 -= (pM - mopt) / 2; }
+            if (pN > nopt) { c0 = (pN - nopt) / 2; c1 -= (pN - nopt) / 2; }
+            if (pP > popt) { e0 = (pP - popt) / 2; e1 -= (pP - popt) / 2; }
+        }
+    }
+    int64_t m = a1 - a0 + 1, n = c1 - c0 + 1, p = e1 - e0 + 1;
+    if (rc == DWCU_SUCCESS) rc = crop(d_psf, pM, pN, a0, c0, e0, m, n, p, sum1, b1);
+    // drop faint outer x and y planes (psf_autocrop_XY)
+    long long first = 0;
+    if (rc == DWCU_SUCCESS && bq > 0 && xycropfactor > 0) {
+        k_psf_plane_sums<<<(int) ((m + 127) / 128), 128, 0, st>>>(b1, m, n, p, plane);
+        k_psf_first_plane<<<1, 32, 0, st>>>(plane, m, xycropfactor, first_d);
+        dwcu::record_launch();
+        dwcu::record_launch();
+        if (cudaGetLastError() != cudaSuccess) rc = fail(DWCU_ERROR_CUDA, "PSF plane-sum launch failed");
+        if (rc == DWCU_SUCCESS &&
+            (cudaMemcpyAsync(&first, first_d, sizeof first, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+             cudaStreamSynchronize(st) != cudaSuccess))
+            rc = fail(DWCU_ERROR_CUDA, "reading the PSF crop failed");
+    }
+    int64_t f = (first >= 1 && m - 2 * first >= 1 && n - 2 * first >= 1) ? first : 0;
+    const int64_t m2 = m - 2 * f, n2 = n - 2 * f;
+    // the cropped PSF, normalised again (dw.c:2826)
+    if (rc == DWCU_SUCCESS) rc = crop(b1, m, n, f, f, 0, m2, n2, p, nullptr, b2);
+    if (rc == DWCU_SUCCESS) rc = dsum(b2, m2 * n2 * p, sum2);
+    if (rc == DWCU_SUCCESS) rc = crop(b2, m2, n2, 0, 0, 0, m2, n2, p, sum2, d_out);
+    if (rc == DWCU_SUCCESS && cudaStreamSynchronize(st) != cudaSuccess)
+        rc = fail(DWCU_ERROR_CUDA, "PSF preparation failed on the device");
+    dims[0] = m2;
+    dims[1] = n2;
+    dims[2] = p;
+    return rc;
+}
+
 }  // namespace dwcu_host
 
 using namespace dwcu_host;
@@ -217,6 +376,17 @@ int dwcu_psf_prepare(const float *psf, int64_t pM, int64_t pN, int64_t pP, int64
     out_dims[1] = pN;
     out_dims[2] = pP;
     return DWCU_SUCCESS;
+}
+
+int dwcu_psf_prepare_device(const float *d_psf, int64_t pM, int64_t pN, int64_t pP, int64_t M, int64_t N,
+                            int64_t P, int32_t border_quality, float xycropfactor, float *d_out, int64_t out_dims[3],
+                            int32_t device, void *stream)
+{
+    if (!d_psf || !d_out || !out_dims) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    if (pM < 1 || pN < 1 || pP < 1 || M < 1 || N < 1 || P < 1) return fail(DWCU_ERROR_INVALID_VALUE, "bad sizes");
+    HCU(cudaSetDevice(device));
+    cudaStream_t st = stream ? (cudaStream_t) stream : cudaStreamPerThread;
+    return psf_prepare_device(d_psf, pM, pN, pP, M, N, P, border_quality, xycropfactor, d_out, out_dims, st);
 }
 
 int dwcu_tiling_create(int64_t M, int64_t N, int64_t P, int64_t max_size, int64_t overlap, dwcu_tile *tiles,
@@ -331,15 +501,32 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, cons
     } joiner{prefault};
 
     // per tile: PSF copy normalised and cropped against the tile
-    // (dw.c:2112-2130); tiles of one size share the result
+    // (dw.c:2112-2130), on the device; tiles of one size share the result
     struct TilePsf {
         int64_t xs[3];
-        std::vector<float> psf;
         int64_t d[3];
         float *dev = nullptr;
     };
     std::vector<TilePsf> psfs;
     std::vector<int> psf_of((size_t) nt);
+    float *d_psf_in = nullptr;
+    auto free_psfs = [&]() {
+        for (auto &tp : psfs)
+            if (tp.dev) cudaFree(tp.dev);
+        if (d_psf_in) cudaFree(d_psf_in);
+        d_psf_in = nullptr;
+    };
+    {
+        cudaError_t e = cudaMalloc(&d_psf_in, sizeof(float) * (size_t) (pM * pN * pP));
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_psf_in, psf, sizeof(float) * (size_t) (pM * pN * pP), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {
+            free_psfs();
+            cleanup();
+            return fail(e == cudaErrorMemoryAllocation ? DWCU_ERROR_OUT_OF_MEMORY : DWCU_ERROR_CUDA,
+                        "PSF upload failed: %s", cudaGetErrorString(e));
+        }
+    }
     for (int i = 0; i < nt; ++i) {
         const dwcu_tile &t = tiles[(size_t) i];
         int k = 0;
@@ -349,31 +536,20 @@ int dwcu_deconvolve_tiled(const float *im, int64_t M, int64_t N, int64_t P, cons
         if (k == (int) psfs.size()) {
             TilePsf tp;
             memcpy(tp.xs, t.xsize, sizeof tp.xs);
-            tp.psf.assign(psf, psf + pM * pN * pP);
-            int64_t a = pM, b = pN, c = pP;
-            normalize_sum1(tp.psf);
-            crop_by_image(tp.psf, a, b, c, t.xsize[0], t.xsize[1], t.xsize[2], s->border_quality);
-            if (s->border_quality > 0 && xycropfactor > 0) crop_xy(tp.psf, a, b, c, xycropfactor);
-            normalize_sum1(tp.psf);
-            tp.d[0] = a; tp.d[1] = b; tp.d[2] = c;
-            psfs.push_back(std::move(tp));
+            int prc = cudaMalloc(&tp.dev, sizeof(float) * (size_t) (pM * pN * pP)) == cudaSuccess
+                          ? DWCU_SUCCESS
+                          : fail(DWCU_ERROR_OUT_OF_MEMORY, "tile PSF buffer");
+            if (prc == DWCU_SUCCESS)
+                prc = psf_prepare_device(d_psf_in, pM, pN, pP, t.xsize[0], t.xsize[1], t.xsize[2], s->border_quality,
+                                         xycropfactor, tp.dev, tp.d, st);
+            psfs.push_back(tp);
+            if (prc != DWCU_SUCCESS) {
+                free_psfs();
+                cleanup();
+                return prc;
+            }
         }
         psf_of[(size_t) i] = k;
-    }
-    auto free_psfs = [&]() {
-        for (auto &tp : psfs)
-            if (tp.dev) cudaFree(tp.dev);
-    };
-    for (auto &tp : psfs) {
-        cudaError_t e = cudaMalloc(&tp.dev, sizeof(float) * tp.psf.size());
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(tp.dev, tp.psf.data(), sizeof(float) * tp.psf.size(), cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) {
-            free_psfs();
-            cleanup();
-            return fail(e == cudaErrorMemoryAllocation ? DWCU_ERROR_OUT_OF_MEMORY : DWCU_ERROR_CUDA,
-                        "tile PSF upload failed: %s", cudaGetErrorString(e));
-        }
     }
     // waves of tiles that fit the device-memory budget, each run as one
     // batch; a tile whose job fills the GPU on its own (>= 32 Mi padded

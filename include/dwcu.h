@@ -173,6 +173,17 @@ int64_t dwcu_job_bytes(const dwcu_job *job);
 int dwcu_psf_prepare(const float *psf, int64_t pM, int64_t pN, int64_t pP,
                      int64_t M, int64_t N, int64_t P, int32_t border_quality,
                      float xycropfactor, float *out, int64_t out_dims[3]);
+/* dwcu_psf_prepare on the device: d_psf (device, pM*pN*pP floats, not
+ * modified) prepared into d_out (device, room for pM*pN*pP floats) with the
+ * same steps and the same float results (the crop decision from float
+ * plane sums in the reference's order; the normalisations' double sums in a
+ * fixed tree).  Work space is allocated and freed inside; returns after
+ * `stream` (NULL: the calling thread's default stream) has drained, with
+ * the new size in out_dims.  The tiled path (dwcu_deconvolve_tiled)
+ * prepares each tile size's PSF with it. */
+int dwcu_psf_prepare_device(const float *d_psf, int64_t pM, int64_t pN, int64_t pP, int64_t M, int64_t N,
+                            int64_t P, int32_t border_quality, float xycropfactor, float *d_out, int64_t out_dims[3],
+                            int32_t device, void *stream);
 
 /* One tile of a tiling (struct tile, src/tiling.h:29-34): the owned region
  * pos = [m0, m1, n0, n1, p0, p1] and the region deconvolved xpos (pos grown
