@@ -45,9 +45,9 @@ def test_device_prepare_equals_host_and_reference(pshape, ishape, bq, xy):
 
 def test_device_prepare_born_wolf():
     from deconwolf_b200 import synthetic
-    for pshape, ishape, lam in (((79, 127, 127), (40, 256, 256), 466.0), ((119, 181, 181), (60, 1124, 1124), 670.0),
-                                ((119, 181, 181), (60, 562, 612), 670.0)):
-        psf = synthetic.bw_psf(pshape, lam=lam)
+    big = synthetic.bw_psf((119, 181, 181), lam=670.0)
+    for psf, ishape in ((synthetic.bw_psf((79, 127, 127), lam=466.0), (40, 256, 256)), (big, (60, 1124, 1124)),
+                        (big, (60, 562, 612))):
         d = _device(psf, ishape, 2, 0.001)
         np.testing.assert_array_equal(d, dw.psf_prepare(psf, ishape, 2, 0.001))
         ref = po.psf_prepare_reference(psf, ishape, 2, 0.001)
