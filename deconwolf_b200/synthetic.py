@@ -91,6 +91,10 @@ CONFIGS = {
     # overlap 50 (1124^2 x 60, job 1344^2 x 180)
     "shb-1124x1124x60": dict(shape=(60, 1124, 1124), psf_shape=(119, 181, 181), lam=670.0, K=12000, B=180,
                              bg=100.0, seed=7),
+    # one tile of the same image at tile size 512 and overlap 50 (612 x 562 x
+    # 60, job 792 x 742 x 178 -> 800 x 750 x 180)
+    "shb-612x562x60": dict(shape=(60, 562, 612), psf_shape=(119, 181, 181), lam=670.0, K=3300, B=50, bg=100.0,
+                           seed=8),
 }
 
 

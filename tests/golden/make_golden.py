@@ -21,8 +21,9 @@ exact relative L2 distance to the FP64 result.
 --config2 (one to two hours on 8 cores, ~20 GB of RAM) runs the reference's
 SHB for 50 iterations on the 2048 x 2048 x 60 workload and stores its trace,
 plane sums, norm, 262144 sampled voxels and a sketch of the whole output.
---tile1024 does the same for one interior tile of the tiled 4096 x 4096 x 60
-workload (1124 x 1124 x 60 with the full PSF).
+--tile1024 and --tile512 do the same for one tile of the tiled 4096 x 4096 x
+60 workload at tile size 1024 (1124 x 1124 x 60) and 512 (612 x 562 x 60),
+with the full PSF.
 """
 from __future__ import annotations
 
@@ -118,22 +119,21 @@ def config2():
         bg=np.float32(r.bg), loop_seconds=np.float64(r.loop_seconds), threads=np.int64(os.cpu_count()))
 
 
-def tile1024():
-    """One interior tile of the 4096 x 4096 x 60 image at tile size 1024 and
-    overlap 50 (1124 x 1124 x 60), with the full 181 x 181 x 119 PSF: the
-    transform lengths of the tiled workload (job 1304 x 1304 x 178, padded on
-    the GPU to 1344 x 1344 x 180), SHB 50 iterations."""
+def tile_golden(name, fixture):
+    """A tile of the 4096 x 4096 x 60 image with the full 181 x 181 x 119 PSF,
+    SHB 50 iterations: 1124 x 1124 x 60 (tile size 1024, overlap 50; job
+    1304 x 1304 x 178, padded on the GPU to 1344 x 1344 x 180) or 612 x 562 x
+    60 (tile size 512; job 792 x 742 x 178 -> 800 x 750 x 180)."""
     from deconwolf_b200 import synthetic
     from tests.helpers import sketch
-    name = "shb-1124x1124x60"
     im, psf = synthetic.config_inputs(name)
     t = time.time()
     r = po.deconvolve(im, psf, method="shb", n_iter=50, impl="reference", threads=os.cpu_count())
-    print("reference SHB 1124x1124x60, 50 it:", time.time() - t, "s", flush=True)
+    print("reference SHB", name, "50 it:", time.time() - t, "s", flush=True)
     idx = np.sort(sample_index(im.shape, 131072))
     out = r.out
     np.savez_compressed(
-        os.path.join(HERE, "tile1024_shb50.npz"),
+        os.path.join(HERE, fixture),
         trace=r.trace, plane_sums=out.astype(np.float64).sum(axis=(1, 2)), sample_idx=idx,
         sample_val=out.reshape(-1)[idx], norm=np.float64(np.linalg.norm(out.astype(np.float64))),
         sketch=sketch(out), image_sum=np.float64(im.astype(np.float64).sum()), image_sample=im.reshape(-1)[idx],
@@ -146,6 +146,7 @@ def main():
     ap.add_argument("--config1-fp64", action="store_true")
     ap.add_argument("--config2", action="store_true")
     ap.add_argument("--tile1024", action="store_true")
+    ap.add_argument("--tile512", action="store_true")
     ap.add_argument("--no-small", action="store_true")
     a = ap.parse_args()
     if not a.no_small:
@@ -160,7 +161,9 @@ def main():
     if a.config2:
         config2()
     if a.tile1024:
-        tile1024()
+        tile_golden("shb-1124x1124x60", "tile1024_shb50.npz")
+    if a.tile512:
+        tile_golden("shb-612x562x60", "tile512_shb50.npz")
 
 
 if __name__ == "__main__":
