@@ -305,7 +305,11 @@ int dwcu_fft_r2c_noalloc(const float *d_in, int64_t M, int64_t N, int64_t P, flo
  * each pass kind on a synthetic volume (CUDA events, a few launches each,
  * milliseconds in all) and keeps the fastest; later jobs use the recorded
  * choice.  The first job of a new size therefore takes a little longer to
- * create, and its creation should not happen during stream capture.
+ * create, and its creation should not happen during stream capture.  The
+ * measurement uses a few hundred MB of device memory of its own (outside a
+ * server's HBM budget), freed right after; freeing waits for the device, so
+ * a serving process that must never stall other streams imports a table
+ * (dwcu_tune_import) or runs dwcu_tune_run for its sizes at start-up.
  * Replaces FFTW's planning by measurement (fft_train, src/fft.c:206-319;
  * FFTW_MEASURE, src/dw.c:400) and its wisdom files (src/fft.c:299-316, 355):
  * dwcu_tune_export writes the table as text, dwcu_tune_import reads it back
