@@ -523,10 +523,16 @@ struct XCfg {
     static constexpr size_t XCH2_BYTES = FAM == 3 ? 0 : sizeof(float2) * (size_t) (R * ROW_F2);
     static constexpr size_t REAL_BYTES = SLOT_BYTES > XCH2_BYTES ? SLOT_BYTES : XCH2_BYTES;
     static constexpr size_t RED_OFF = REAL_OFF + (REAL_BYTES + 7) / 8 * 8;
-    static constexpr size_t SMEM_BYTES = RED_OFF + sizeof(double) * THREADS;
-    // resident CTAs per SM to aim for (registers are capped to fit them)
-    // (one-row update tiles, family 2: five CTAs, which caps registers at 72)
-    static constexpr int MIN_BLOCKS = (R == 1 && FAM == 2 && SMEM_BYTES * 5 <= 224 * 1024 && THREADS * 5 <= 2048) ? 5
+    // the error partials' reduction area: ratio family only
+    static constexpr size_t SMEM_BYTES = RED_OFF + (FAM == 1 ? sizeof(double) * THREADS : 0);
+    // resident CTAs per SM to aim for (registers are capped to fit them):
+    // one-row update tiles of at most five warps take six where their shared
+    // memory (plus the 1 KB the hardware reserves per block) fits, which
+    // leaves 64 registers a thread (x 2240: no spills; 4.80 -> 4.65 ms per
+    // update pass against five), else five
+    static constexpr int MIN_BLOCKS =
+        (R == 1 && FAM == 2 && THREADS <= 160 && (SMEM_BYTES + 1024) * 6 <= 228 * 1024) ? 6
+        : (R == 1 && FAM == 2 && SMEM_BYTES * 5 <= 224 * 1024 && THREADS * 5 <= 2048) ? 5
                                     : (SMEM_BYTES * 4 <= 224 * 1024 && THREADS * 4 <= 2048) ? 4
                                     : (SMEM_BYTES * 3 <= 225 * 1024 && THREADS * 3 <= 2048) ? 3 : 1;
     static_assert(R % Q == 0, "rows per tile");
