@@ -642,8 +642,12 @@ __device__ __forceinline__ void x_row_op(const XArgs &a, int op, int t, long lon
             const float v0 = img0 ? g0 / d0 : 0.f;
             const float v1 = img1 ? g1 / d1 : 0.f;
             // the error's g/y is the same quotient unless the guard changed y
-            if (img0) acc += err_term_q(y0, g0, d0 == y0 ? v0 : g0 / y0, a.metric);
-            if (img1) acc += err_term_q(y1, g1, d1 == y1 ? v1 : g1 / y1, a.metric);
+            // (a branch, so that the second division runs only then)
+            float q0 = v0, q1 = v1;
+            if (d0 != y0) q0 = g0 / y0;
+            if (d1 != y1) q1 = g1 / y1;
+            if (img0) acc += err_term_q(y0, g0, q0, a.metric);
+            if (img1) acc += err_term_q(y1, g1, q1, a.metric);
             w[r] = make_float2(v0, v1);
         }
         break;
