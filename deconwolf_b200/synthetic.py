@@ -179,6 +179,14 @@ def synth_image_blocked(shape, psf: np.ndarray, K: int, B: int, bg: float, seed:
     return out
 
 
+def _save_atomic(path: str, a: np.ndarray) -> None:
+    """np.save through a private temporary file and a rename, so that
+    processes sharing the cache (one per GPU) never read a partial file."""
+    tmp = f"{path}.{os.getpid()}.tmp.npy"
+    np.save(tmp, a)
+    os.replace(tmp, path)
+
+
 def cached(name: str, cache_dir: str | None, make):
     """(image, psf) from ``make()``, cached as .npy under cache_dir."""
     if cache_dir:
@@ -189,8 +197,8 @@ def cached(name: str, cache_dir: str | None, make):
             return np.load(fi), np.load(fp)
     im, psf = make()
     if cache_dir:
-        np.save(fi, im)
-        np.save(fp, psf)
+        _save_atomic(fi, im)
+        _save_atomic(fp, psf)
     return im, psf
 
 
@@ -272,7 +280,7 @@ def serve_psf(size: int, lam: float, cache_dir: str | None = None) -> np.ndarray
     psf = bw_psf((2 * P - 1, 181, 181), lam=lam)
     if cache_dir:
         os.makedirs(cache_dir, exist_ok=True)
-        np.save(f, psf)
+        _save_atomic(f, psf)
     return psf
 
 
@@ -289,6 +297,6 @@ def config_inputs(name: str, cache_dir: str | None = None):
     psf = bw_psf(c["psf_shape"], lam=c["lam"])
     im = synth_image(c["shape"], psf, c["K"], c["B"], c["bg"], c["seed"])
     if cache_dir:
-        np.save(fi, im)
-        np.save(fp, psf)
+        _save_atomic(fi, im)
+        _save_atomic(fp, psf)
     return im, psf
