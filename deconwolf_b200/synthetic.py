@@ -212,6 +212,17 @@ def tiled_inputs(cache_dir: str | None = None):
     return cached("tiles-4096x4096x60", cache_dir, make)
 
 
+def tiled_pair_inputs(cache_dir: str | None = None):
+    """A 2048 x 1024 x 60 image that tiling splits into two tiles at tile
+    size 1024 and overlap 50: the generator of the 2048 x 2048 x 60 workload
+    scaled by area (K = 20000, B = 300), seed 9; PSF Born-Wolf 670 nm
+    181 x 181 x 119."""
+    def make():
+        psf = bw_psf((119, 181, 181), lam=670.0)
+        return synth_image_blocked((60, 1024, 2048), psf, 20000, 300, 100.0, 9), psf
+    return cached("tiles-2048x1024x60", cache_dir, make)
+
+
 CHANNEL_LAMBDAS = (405.0, 466.0, 525.0, 595.0, 670.0, 750.0)
 CHANNEL_ITERS = (20, 40, 60, 80, 100, 150)
 

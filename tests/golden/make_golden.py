@@ -24,6 +24,9 @@ plane sums, norm, 262144 sampled voxels and a sketch of the whole output.
 --tile1024 and --tile512 do the same for one tile of the tiled 4096 x 4096 x
 60 workload at tile size 1024 (1124 x 1124 x 60) and 512 (612 x 562 x 60),
 with the full PSF.
+
+--tiled-pair runs the reference's tiled path (tiling.c, per-tile PSF crop,
+weighted blend) on a 2048 x 1024 x 60 image at tile size 1024 (two tiles).
 """
 from __future__ import annotations
 
@@ -140,6 +143,27 @@ def tile_golden(name, fixture):
         bg=np.float32(r.bg), loop_seconds=np.float64(r.loop_seconds), threads=np.int64(os.cpu_count()))
 
 
+def tiled_pair():
+    """The reference's tiled path (deconvolve_tiles over tiling.c, each tile
+    with its own PSF crop, weighted blend) on the 2048 x 1024 x 60 image at
+    tile size 1024, overlap 50 (two tiles), SHB 50 iterations; the PSF
+    prepared for the whole image as dw_run does."""
+    from deconwolf_b200 import synthetic
+    from tests.helpers import sketch
+    im, psf = synthetic.tiled_pair_inputs()
+    pp = po.psf_prepare_reference(psf, im.shape)
+    t = time.time()
+    r = po.deconvolve_tiled(im, pp, 1024, 50, method="shb", n_iter=50, impl="reference", threads=os.cpu_count())
+    print("reference tiled SHB 2048x1024x60, 50 it:", time.time() - t, "s", flush=True)
+    idx = np.sort(sample_index(im.shape, 131072))
+    out = r.out
+    np.savez_compressed(
+        os.path.join(HERE, "tiled2_shb50.npz"),
+        plane_sums=out.astype(np.float64).sum(axis=(1, 2)), sample_idx=idx, sample_val=out.reshape(-1)[idx],
+        norm=np.float64(np.linalg.norm(out.astype(np.float64))), sketch=sketch(out),
+        image_sample=im.reshape(-1)[idx], psf_shape=np.array(pp.shape), threads=np.int64(os.cpu_count()))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--config1", action="store_true")
@@ -147,6 +171,7 @@ def main():
     ap.add_argument("--config2", action="store_true")
     ap.add_argument("--tile1024", action="store_true")
     ap.add_argument("--tile512", action="store_true")
+    ap.add_argument("--tiled-pair", action="store_true")
     ap.add_argument("--no-small", action="store_true")
     a = ap.parse_args()
     if not a.no_small:
@@ -164,6 +189,8 @@ def main():
         tile_golden("shb-1124x1124x60", "tile1024_shb50.npz")
     if a.tile512:
         tile_golden("shb-612x562x60", "tile512_shb50.npz")
+    if a.tiled_pair:
+        tiled_pair()
 
 
 if __name__ == "__main__":

@@ -116,3 +116,29 @@ def test_multi_layer_single_rank_equals_batched():
     res = multi.run_jobs(jobs)
     for j, r in zip(jobs, res):
         np.testing.assert_array_equal(r, dw.run_method(j["image"], j["psf"], **j["kw"]).out)
+
+
+def test_tiled_pair_golden():
+    """The tiled path at full size: a 2048 x 1024 x 60 image at tile size 1024
+    and overlap 50 (two tiles of 1074-1124 x 1024 x 60, each with its own PSF
+    crop, weighted blend), SHB 50, against the reference's own tiled path
+    (tiling.c with the reference's method code): every plane sum, the norm,
+    131072 sampled voxels and the whole-volume sketch."""
+    import os
+    f = os.path.join(os.path.dirname(__file__), "golden", "tiled2_shb50.npz")
+    if not os.path.exists(f):
+        pytest.skip("tiled fixture not generated")
+    from deconwolf_b200 import synthetic
+    from tests.helpers import sketch, sketch_rel_l2
+    d = np.load(f)
+    im, psf = synthetic.tiled_pair_inputs()
+    idx = d["sample_idx"]
+    np.testing.assert_array_equal(im.reshape(-1)[idx], d["image_sample"])
+    pp = dw.psf_prepare(psf, im.shape)
+    assert tuple(pp.shape) == tuple(d["psf_shape"])
+    g = dw.deconvolve_tiled(im, pp, 1024, 50, method="shb", n_iter=50)
+    assert rel_l2(g.out.reshape(-1)[idx], d["sample_val"]) < OUT_TOL
+    assert rel_l2(g.out.astype(np.float64).sum(axis=(1, 2)), d["plane_sums"]) < OUT_TOL
+    est = sketch_rel_l2(sketch(g.out, device="cuda"), d["sketch"], float(d["norm"]))
+    print(f"\ntiled 2048x1024x60 (2 tiles): relative L2 to the reference tiled path (sketch) {est:.3e}")
+    assert est < OUT_TOL
