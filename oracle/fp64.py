@@ -144,3 +144,80 @@ def deconvolve_fp64(im: np.ndarray, psf: np.ndarray, method: str = "shb", n_iter
     # RL the newest one (method_rl.c:393)
     res = xp if shb else x
     return Fp64Result(np.ascontiguousarray(res[img]), trace, float(bg), w)
+
+
+def deconvolve_fp64_torch(im: np.ndarray, psf: np.ndarray, method: str = "shb", n_iter: int = 50, bq: int = 2,
+                          bg: float | None = None, positivity: bool = True, alphamax: float = 1.0,
+                          device: str = "cpu") -> Fp64Result:
+    """deconvolve_fp64 with torch float64 tensors and transforms (on ``device``,
+    e.g. a GPU for volumes too large for host memory in float64); the same
+    steps, flat start, I-divergence.  Returns the result on the host."""
+    import torch
+    g = torch.as_tensor(np.asarray(im, dtype=np.float64), device=device)
+    P, N, M = g.shape
+    if n_iter == 0:
+        return Fp64Result(g.cpu().numpy(), np.zeros(0), float(bg or 0), tuple(g.shape))
+    if bg is None:
+        bg = max(float(g.min()), 0.01)
+    w = job_size(tuple(g.shape), psf.shape, bq)
+    Z = torch.zeros(w, dtype=torch.float64, device=device)
+    pP, pN, pM = psf.shape
+    Z[:pP, :pN, :pM] = torch.as_tensor(np.asarray(psf, dtype=np.float64), device=device)
+    c, b, a = np.unravel_index(int(torch.argmax(Z).item()), w)
+    Z = torch.roll(Z, shifts=(-int(c), -int(b), -int(a)), dims=(0, 1, 2))
+    K = torch.fft.rfftn(Z)
+    del Z
+    Kc = torch.conj(K)
+
+    def conv(X, H):
+        return torch.fft.irfftn(torch.fft.rfftn(X) * H, s=w)
+
+    W = None
+    if bq > 0:
+        one = torch.zeros(w, dtype=torch.float64, device=device)
+        one[:P, :N, :M] = 1.0
+        P1 = conv(one, Kc)
+        del one
+        W = torch.where(P1 > 0.01, 1.0 / torch.where(P1 > 0.01, P1, torch.ones_like(P1)), torch.zeros_like(P1))
+        del P1
+    x = torch.full(w, float(g.sum().item()) / float(np.prod(w)), dtype=torch.float64, device=device)
+    xp = x.clone()
+    trace = np.zeros(n_iter)
+    shb = method == "shb"
+
+    def idiv(ys):
+        m = (ys > 0) & (g > 0)
+        gm, ym = g[m], ys[m]
+        return float(((gm * torch.log(gm / ym)) - (gm - ym)).sum().item() / g.numel())
+
+    for it in range(n_iter):
+        if shb:
+            alpha = min(max((it - 1.0) / (it + 2.0), 0.0), alphamax)
+            p = torch.clamp(x + alpha * (x - xp), min=bg)
+            y = conv(p, K)
+            ys = y[:P, :N, :M]
+            trace[it] = idiv(ys)
+            ys = torch.where(ys.abs() < 1e-6, torch.copysign(torch.full_like(ys, 1e-6), ys), ys)
+            r = torch.zeros(w, dtype=torch.float64, device=device)
+            r[:P, :N, :M] = g / ys
+            del y, ys
+            xn = conv(r, Kc) * (p * W if W is not None else p)
+            del r, p
+            xp, x = x, xn
+            if positivity:
+                x = torch.clamp(x, min=bg)
+        else:
+            f = x
+            y = conv(f, K)
+            ys = y[:P, :N, :M]
+            trace[it] = idiv(ys)
+            r = torch.full(w, 1e-6, dtype=torch.float64, device=device)
+            pos = ys > 0
+            r[:P, :N, :M] = torch.where(pos, g / torch.where(pos, ys, torch.ones_like(ys)), torch.full_like(ys, bg))
+            del y, ys
+            xn = conv(r, Kc) * (f * W if W is not None else f)
+            if bg > 0:
+                xn = torch.clamp(xn, min=bg)
+            x = xn
+    res = xp if shb else x
+    return Fp64Result(res[:P, :N, :M].contiguous().cpu().numpy(), trace, float(bg), w)

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from oracle import pyoracle as po
-from oracle.fp64 import deconvolve_fp64, job_size
+from oracle.fp64 import deconvolve_fp64, deconvolve_fp64_torch, job_size
 from tests.helpers import gauss_psf, poisson_image, rel_l2, sketch, sketch_rel_l2
 
 pytestmark = pytest.mark.skipif(not po.available("port"), reason="oracle not built (make -C oracle)")
@@ -91,3 +91,14 @@ def test_sketch_estimates_relative_l2():
         assert 0.6 < est / true < 1.5
     # exact zero distance
     assert sketch_rel_l2(sketch(b), sketch(b.copy()), 1.0) == 0.0
+
+
+@pytest.mark.parametrize("method,bq", [("shb", 2), ("rl", 2), ("shb", 1), ("rl", 0)])
+def test_torch_twin_equals_numpy(method, bq):
+    """The torch form (used on the GPU for volumes too large for host memory
+    in float64) takes the same steps: equal to rounding in float64."""
+    im, psf = _inputs(3, (9, 22, 19), (5, 7, 9))
+    a = deconvolve_fp64(im, psf, method=method, n_iter=15, bq=bq)
+    b = deconvolve_fp64_torch(im, psf, method=method, n_iter=15, bq=bq)
+    assert np.max(np.abs(a.out - b.out)) <= 1e-12 * np.max(np.abs(a.out))
+    assert np.max(np.abs(a.trace - b.trace) / a.trace) < 1e-12

@@ -19,7 +19,7 @@ import pytest
 
 import deconwolf_b200 as dw
 from oracle import pyoracle as po
-from oracle.fp64 import deconvolve_fp64
+from oracle.fp64 import deconvolve_fp64, deconvolve_fp64_torch
 from tests.helpers import gauss_psf, poisson_image, rel_l2, sketch, sketch_rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -80,3 +80,32 @@ def test_config1_error_against_fp64():
     assert e_gpu_sk <= FP64_FACTOR * max(e_ref, FP64_FLOOR)
     assert e_gpu_sm <= FP64_FACTOR * max(e_ref, FP64_FLOOR)
     assert t_gpu <= FP64_FACTOR * max(float(d["ref_trace_rel_fp64"]), FP64_FLOOR)
+
+
+def test_config2_error_against_fp64():
+    """2048 x 2048 x 60, SHB 50: the FP64 run of the same iteration on the GPU
+    (torch float64, the same steps as the NumPy restatement), the GPU
+    result's exact distance to it over the whole volume, and the reference's
+    distance from its fixture (sketch and samples)."""
+    f = os.path.join(os.path.dirname(__file__), "golden", "config2_shb50.npz")
+    if not os.path.exists(f):
+        pytest.skip("config2 fixture not generated")
+    from deconwolf_b200 import synthetic
+    d = np.load(f)
+    im, psf = synthetic.config_inputs("shb-2048x2048x60")
+    g = dw.run_method(im, psf, method="shb", n_iter=50)
+    dw.release_cache()  # the engine's cached 19 GB block: the float64 run needs the room
+    fr = deconvolve_fp64_torch(im, psf, method="shb", n_iter=50, device="cuda")
+    import torch
+    torch.cuda.empty_cache()
+    e_gpu = rel_l2(g.out, fr.out)
+    norm64 = float(np.linalg.norm(fr.out))
+    e_ref_sk = sketch_rel_l2(d["sketch"], sketch(fr.out, device="cuda"), norm64)
+    idx = d["sample_idx"]
+    e_ref_sm = rel_l2(d["sample_val"], fr.out.reshape(-1)[idx])
+    t_gpu = float(np.max(np.abs(g.trace - fr.trace) / fr.trace))
+    t_ref = float(np.max(np.abs(d["trace"] - fr.trace) / fr.trace))
+    print(f"\nFP64 distance config 2: GPU {e_gpu:.3e} (exact, whole volume), trace {t_gpu:.2e}; "
+          f"reference {e_ref_sk:.3e} (sketch), {e_ref_sm:.3e} (samples), trace {t_ref:.2e}")
+    assert e_gpu <= FP64_FACTOR * max(e_ref_sk, FP64_FLOOR)
+    assert t_gpu <= FP64_FACTOR * max(t_ref, FP64_FLOOR)
