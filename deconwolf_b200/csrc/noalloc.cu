@@ -16,7 +16,8 @@
 //     (spectrum + staged input + scalars + twiddle tables, see need_bytes)
 //     are rejected with DWCU_ERROR_INVALID_VALUE;
 //   * the first call on a device does one-time setup (the symbol lookup,
-//     which loads this module, and the kernels' shared-memory attributes);
+//     which loads this module, and the kernels' shared-memory attributes),
+//     so that first call belongs before any stream capture;
 //   * the spectrum, the staged input and the error flags must start at zero:
 //     every call clears them on its stream before the transform;
 //   * there is one work space per device, so two calls that overlapped on one

@@ -286,9 +286,12 @@ int dwcu_fft_c2r(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_ou
  * device-wide synchronisation of cudaFree while other streams of the GPU are
  * busy.  Transforms whose spectrum, staged input and twiddle tables need more
  * than the work space are rejected with DWCU_ERROR_INVALID_VALUE.  The first
- * call on a device does one-time setup (symbol lookup, kernel attributes).
- * Calls on one device share the work space: they are serialised by a lock
- * and each returns after its stream has drained.  A NULL stream means the
+ * call on a device does one-time setup (symbol lookup, kernel attributes),
+ * so make that first call before any stream capture.  Calls on one device
+ * share the work space, which keeps the last call's contents (each call
+ * clears the parts that must start at zero); two calls whose GPU work
+ * overlapped would race on it, so calls are serialised by a lock and each
+ * returns after its stream has drained.  A NULL stream means the
  * calling thread's default stream (cudaStreamPerThread); pass a stream of
  * your own to keep the transform beside other work.  The caller's current
  * device is left as it was. */
