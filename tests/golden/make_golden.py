@@ -25,6 +25,8 @@ plane sums, norm, 262144 sampled voxels and a sketch of the whole output.
 60 workload at tile size 1024 (1124 x 1124 x 60) and 512 (612 x 562 x 60),
 with the full PSF.
 
+--tile512-rl is the 612 x 562 x 60 tile with RL instead of SHB.
+
 --tiled-pair runs the reference's tiled path (tiling.c, per-tile PSF crop,
 weighted blend) on a 2048 x 1024 x 60 image at tile size 1024 (two tiles).
 """
@@ -122,7 +124,7 @@ def config2():
         bg=np.float32(r.bg), loop_seconds=np.float64(r.loop_seconds), threads=np.int64(os.cpu_count()))
 
 
-def tile_golden(name, fixture):
+def tile_golden(name, fixture, method="shb"):
     """A tile of the 4096 x 4096 x 60 image with the full 181 x 181 x 119 PSF,
     SHB 50 iterations: 1124 x 1124 x 60 (tile size 1024, overlap 50; job
     1304 x 1304 x 178, padded on the GPU to 1344 x 1344 x 180) or 612 x 562 x
@@ -131,8 +133,8 @@ def tile_golden(name, fixture):
     from tests.helpers import sketch
     im, psf = synthetic.config_inputs(name)
     t = time.time()
-    r = po.deconvolve(im, psf, method="shb", n_iter=50, impl="reference", threads=os.cpu_count())
-    print("reference SHB", name, "50 it:", time.time() - t, "s", flush=True)
+    r = po.deconvolve(im, psf, method=method, n_iter=50, impl="reference", threads=os.cpu_count())
+    print("reference", method, name, "50 it:", time.time() - t, "s", flush=True)
     idx = np.sort(sample_index(im.shape, 131072))
     out = r.out
     np.savez_compressed(
@@ -172,6 +174,7 @@ def main():
     ap.add_argument("--tile1024", action="store_true")
     ap.add_argument("--tile512", action="store_true")
     ap.add_argument("--tiled-pair", action="store_true")
+    ap.add_argument("--tile512-rl", action="store_true")
     ap.add_argument("--no-small", action="store_true")
     a = ap.parse_args()
     if not a.no_small:
@@ -191,6 +194,8 @@ def main():
         tile_golden("shb-612x562x60", "tile512_shb50.npz")
     if a.tiled_pair:
         tiled_pair()
+    if a.tile512_rl:
+        tile_golden("shb-612x562x60", "tile512_rl50.npz", method="rl")
 
 
 if __name__ == "__main__":

@@ -192,11 +192,12 @@ def test_config2_golden():
     assert est < OUT_TOL
 
 
-@pytest.mark.parametrize("name,fixture,work", [
-    ("shb-1124x1124x60", "tile1024_shb50.npz", (1344, 1344, 180)),
-    ("shb-612x562x60", "tile512_shb50.npz", (800, 750, 180)),
+@pytest.mark.parametrize("name,fixture,work,method", [
+    ("shb-1124x1124x60", "tile1024_shb50.npz", (1344, 1344, 180), "shb"),
+    ("shb-612x562x60", "tile512_shb50.npz", (800, 750, 180), "shb"),
+    ("shb-612x562x60", "tile512_rl50.npz", (800, 750, 180), "rl"),
 ])
-def test_tile_golden(name, fixture, work):
+def test_tile_golden(name, fixture, work, method):
     """Tiles of the 4096 x 4096 x 60 image at tile size 1024 (1124 x 1124 x
     60, job 1304 x 1304 x 178 -> 1344 x 1344 x 180) and 512 (612 x 562 x 60,
     job 792 x 742 x 178 -> 800 x 750 x 180), full 181 x 181 x 119 PSF: the
@@ -211,13 +212,13 @@ def test_tile_golden(name, fixture, work):
     im, psf = synthetic.config_inputs(name)
     idx = d["sample_idx"]
     np.testing.assert_array_equal(im.reshape(-1)[idx], d["image_sample"])
-    g = dw.run_method(im, psf, method="shb", n_iter=50)
+    g = dw.run_method(im, psf, method=method, n_iter=50)
     assert g.work == work
     assert trace_err(g.trace, d["trace"]) < TRACE_TOL
     assert rel_l2(g.out.reshape(-1)[idx], d["sample_val"]) < OUT_TOL
     assert rel_l2(g.out.astype(np.float64).sum(axis=(1, 2)), d["plane_sums"]) < OUT_TOL
     est = sketch_rel_l2(sketch(g.out, device="cuda"), d["sketch"], float(d["norm"]))
-    print(f"\n{name}: relative L2 to the reference over the volume (sketch) {est:.3e}, "
+    print(f"\n{name} {method}: relative L2 to the reference over the volume (sketch) {est:.3e}, "
           f"trace {trace_err(g.trace, d['trace']):.2e}")
     assert est < OUT_TOL
 
