@@ -128,7 +128,7 @@ EXPORTS = [
     "dwcu_server_destroy", "dwcu_tile_blend", "dwcu_release_cache",
     "dwcu_tune_set_mode", "dwcu_tune_get_mode", "dwcu_tune_select", "dwcu_tune_plan_count",
     "dwcu_tune_plan_info", "dwcu_tune_force", "dwcu_tune_run", "dwcu_tune_query", "dwcu_tune_clear",
-    "dwcu_tune_export", "dwcu_tune_import", "dwcu_psf_prepare_device",
+    "dwcu_tune_export", "dwcu_tune_import", "dwcu_psf_prepare_device", "dwcu_selftest_bounded_wait",
 ]
 
 # pass kinds of the autotuner (dwcu.h)
@@ -218,6 +218,8 @@ def lib() -> ctypes.CDLL:
                L.dwcu_tune_plan_info, L.dwcu_tune_force, L.dwcu_tune_run, L.dwcu_tune_query, L.dwcu_tune_clear,
                L.dwcu_tune_export, L.dwcu_tune_import):
         fn.restype = ctypes.c_int
+    L.dwcu_selftest_bounded_wait.argtypes = [i32, i32, ctypes.c_uint32]
+    L.dwcu_selftest_bounded_wait.restype = ctypes.c_int
     L.dwcu_psf_prepare_device.argtypes = [vp, i64, i64, i64, i64, i64, i64, i32, ctypes.c_float, vp,
                                           ctypes.POINTER(i64), i32, vp]
     L.dwcu_psf_prepare_device.restype = ctypes.c_int

@@ -1907,6 +1907,50 @@ int dwcu_device_count(void)
 }
 int64_t dwcu_launch_count(void) { return g_launches; }
 
+}  // extern "C"
+
+namespace dwcu {
+// The bounded-wait path of the passes (wait_all), exercised on its own: one
+// block waits on an mbarrier phase that only completes when `arrive` is set
+// (no copy is ever issued, so nothing is in flight when the block leaves).
+__global__ void k_wait_selftest(int *err, unsigned polls, int arrive)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (arrive && threadIdx.x == 0) mbar_arrive(&bar);
+    wait_all(&bar, 0, err, 1 << 8, polls);
+}
+}  // namespace dwcu
+
+extern "C" {
+
+int dwcu_selftest_bounded_wait(int32_t device, int32_t arrive, uint32_t polls)
+{
+    if (polls < 1) return fail(DWCU_ERROR_INVALID_VALUE, "polls must be positive");
+    DeviceCtx *ctx = nullptr;
+    TRY(get_ctx(device, &ctx));
+    CU(cudaSetDevice(device));
+    int *d_flag = nullptr;
+    CU(cudaMalloc(&d_flag, sizeof(int)));
+    int h_flag = 0;
+    cudaError_t e = cudaMemsetAsync(d_flag, 0, sizeof(int), ctx->stream);
+    if (e == cudaSuccess) {
+        k_wait_selftest<<<1, 64, 0, ctx->stream>>>(d_flag, polls, arrive ? 1 : 0);
+        ++g_launches;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_flag);
+    if (e != cudaSuccess) return fail(DWCU_ERROR_CUDA, "bounded-wait self-test failed: %s", cudaGetErrorString(e));
+    if (h_flag & ~0xff) return fail(DWCU_ERROR_TIMEOUT, "a bounded wait gave up after %u polls", polls);
+    return DWCU_SUCCESS;
+}
+
 int dwcu_profile_enable(int32_t on)
 {
     std::lock_guard<std::mutex> lk(g_prof_mu);

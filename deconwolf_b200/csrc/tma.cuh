@@ -42,6 +42,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // 1-D bulk copy global -> shared; bytes and both addresses multiples of 16
 __device__ __forceinline__ void tma_load_1d(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
@@ -68,11 +73,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 // Bounded wait on a barrier phase by every thread of the block, followed by
 // a block-wide vote: returns true on all threads, or false on all threads
 // when any of them gave up (the caller then skips the rest of its work).
-__device__ __forceinline__ bool wait_all(uint64_t *bar, uint32_t parity, int *err_flag, int code)
+__device__ __forceinline__ bool wait_all(uint64_t *bar, uint32_t parity, int *err_flag, int code,
+                                         unsigned limit = kWaitLimit)
 {
     unsigned n = 0;
     bool ok = false;
-    while (n < kWaitLimit) {
+    while (n < limit) {
         if (mbar_try_wait(bar, parity)) {
             ok = true;
             break;

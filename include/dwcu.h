@@ -370,6 +370,15 @@ int dwcu_abi_version(void);
 int dwcu_device_count(void);
 /* Number of kernel launches this thread has issued through the library. */
 int64_t dwcu_launch_count(void);
+/* Self-test of the device-side bounded waits every pass uses (TMA copies
+ * complete on mbarriers; a wait that runs out of polls sets an error word,
+ * the block leaves through one exit, and the host turns the word into
+ * DWCU_ERROR_TIMEOUT): one block waits at most `polls` polls on a barrier
+ * phase that completes only when `arrive` is non-zero.  Returns
+ * DWCU_SUCCESS when the phase completed, DWCU_ERROR_TIMEOUT when the wait
+ * gave up; the device stays usable either way.  No counterpart in the
+ * reference, which exits on any device error. */
+int dwcu_selftest_bounded_wait(int32_t device, int32_t arrive, uint32_t polls);
 
 #ifdef __cplusplus
 }
