@@ -129,6 +129,7 @@ EXPORTS = [
     "dwcu_tune_set_mode", "dwcu_tune_get_mode", "dwcu_tune_select", "dwcu_tune_plan_count",
     "dwcu_tune_plan_info", "dwcu_tune_force", "dwcu_tune_run", "dwcu_tune_query", "dwcu_tune_clear",
     "dwcu_tune_export", "dwcu_tune_import", "dwcu_psf_prepare_device", "dwcu_selftest_bounded_wait",
+    "dwcu_debug_guards", "dwcu_debug_guard_violations",
 ]
 
 # pass kinds of the autotuner (dwcu.h)
@@ -218,6 +219,10 @@ def lib() -> ctypes.CDLL:
                L.dwcu_tune_plan_info, L.dwcu_tune_force, L.dwcu_tune_run, L.dwcu_tune_query, L.dwcu_tune_clear,
                L.dwcu_tune_export, L.dwcu_tune_import):
         fn.restype = ctypes.c_int
+    L.dwcu_debug_guards.argtypes = [i32]
+    L.dwcu_debug_guards.restype = ctypes.c_int
+    L.dwcu_debug_guard_violations.argtypes = []
+    L.dwcu_debug_guard_violations.restype = i64
     L.dwcu_selftest_bounded_wait.argtypes = [i32, i32, ctypes.c_uint32]
     L.dwcu_selftest_bounded_wait.restype = ctypes.c_int
     L.dwcu_psf_prepare_device.argtypes = [vp, i64, i64, i64, i64, i64, i64, i32, ctypes.c_float, vp,

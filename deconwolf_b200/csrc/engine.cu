@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -557,6 +558,7 @@ struct dwcu_job {
     bool loop_started = false;
     cudaGraphExec_t graph = nullptr; // a graph owned by this job (holding timing events)
     double enqueue_s = 0;          // host time inside job_step
+    std::vector<size_t> guards;    // offsets of the guard bands in the block (debug mode)
 };
 
 namespace dwcu {
@@ -800,9 +802,24 @@ static int iter_input(dwcu_job *j, int k)
     return pass_x(j, XOP_FWD_COPY, 1, j->S, j->xa, nullptr, nullptr, 0, 0);
 }
 
+// ------------------------------------------------------------ guard bands
+//
+// A debugging aid in place of a memory checker: with guards on, every region
+// of a job's block is preceded (and the last one followed) by kGuardBytes of
+// a fixed pattern, written when the job is created and compared when it is
+// destroyed; a write past the end of a region, or before its start, shows up
+// as a changed guard (counted, and reported on stderr).  Mode 2 also
+// overwrites one byte of the first guard from the host after filling it, so
+// that a test can see the check find a change.
+static std::atomic<int> g_guard_mode{0};
+static std::atomic<long long> g_guard_violations{0};
+constexpr size_t kGuardBytes = 4096;
+constexpr int kGuardByte = 0xA5;
+
 static int alloc_job(dwcu_job *j)
 {
     const Geometry &g = j->g;
+    const int guard_mode = g_guard_mode.load();
     // the x pass stages R rows per tile; a partial last tile reads (and
     // never uses) one row past the end, so every staged array gets a spare row
     const size_t R = sizeof(float) * (size_t) (g.real_elems() + g.XP);
@@ -814,7 +831,16 @@ static int alloc_job(dwcu_job *j)
     j->n_apart = (int) std::min<long long>(1024, (npsf + 4095) / 4096);
     const bool need_w = j->s.border_quality > 0;
     size_t off = 0;
-    auto take = [&](size_t b) { size_t o = off; off += align256(b); return o; };
+    j->guards.clear();
+    auto take = [&](size_t b) {
+        if (guard_mode) {
+            j->guards.push_back(off);
+            off += kGuardBytes;
+        }
+        size_t o = off;
+        off += align256(b);
+        return o;
+    };
     size_t o_g = take(G), o_S = take(C), o_K = take(C), o_xa = take(R), o_xb = take(R);
     size_t o_W = need_w ? take(R) : 0;
     size_t o_part = take(sizeof(double) * (size_t) j->nxb);
@@ -824,6 +850,10 @@ static int alloc_job(dwcu_job *j)
     size_t o_sp = take(sizeof(StatsPartial) * (size_t) j->n_spart);
     size_t o_ap = take(sizeof(ArgmaxPartial) * (size_t) j->n_apart);
     size_t o_psf = take(sizeof(float) * (size_t) npsf);
+    if (guard_mode) {
+        j->guards.push_back(off);
+        off += kGuardBytes;
+    }
     j->bytes = off;
     j->block = block_get(j->s.device, off);
     if (!j->block)
@@ -843,7 +873,32 @@ static int alloc_job(dwcu_job *j)
     j->spart = (StatsPartial *) (b + o_sp);
     j->apart = (ArgmaxPartial *) (b + o_ap);
     j->psf_dev = (float *) (b + o_psf);
+    for (size_t go : j->guards)
+        if (cudaMemsetAsync(b + go, kGuardByte, kGuardBytes, j->stream) != cudaSuccess)
+            return fail(DWCU_ERROR_CUDA, "filling a guard band failed");
+    if (guard_mode == 2 && !j->guards.empty() && cudaMemsetAsync(b + j->guards[0], 0, 1, j->stream) != cudaSuccess)
+        return fail(DWCU_ERROR_CUDA, "marking a guard band failed");
     return DWCU_SUCCESS;
+}
+
+// compares the job's guard bands with the pattern (after its work is done)
+static void check_guards(dwcu_job *j)
+{
+    if (j->guards.empty() || !j->base) return;
+    std::vector<unsigned char> h(kGuardBytes);
+    for (size_t i = 0; i < j->guards.size(); ++i) {
+        if (cudaMemcpy(h.data(), j->base + j->guards[i], kGuardBytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        size_t bad = 0;
+        for (unsigned char c : h) bad += (c != (unsigned char) kGuardByte);
+        if (bad) {
+            ++g_guard_violations;
+            fprintf(stderr, "dwcu: guard band %zu of a %lld x %lld x %lld job changed (%zu bytes)\n", i,
+                    (long long) j->g.M, (long long) j->g.N, (long long) j->g.P, bad);
+        }
+    }
 }
 
 // ------------------------------------------------------------ autotuning
@@ -1865,6 +1920,7 @@ void dwcu_job_destroy(dwcu_job *j)
     if (!j) return;
     cudaSetDevice(j->s.device);
     if (j->stream) cudaStreamSynchronize(j->stream);
+    check_guards(j);
     if (j->graph) cudaGraphExecDestroy(j->graph);
     if (j->block) block_put(j->block);
     if (j->ev0) cudaEventDestroy(j->ev0);
@@ -1927,6 +1983,15 @@ __global__ void k_wait_selftest(int *err, unsigned polls, int arrive)
 }  // namespace dwcu
 
 extern "C" {
+
+int dwcu_debug_guards(int32_t mode)
+{
+    if (mode < 0 || mode > 2) return fail(DWCU_ERROR_INVALID_VALUE, "guard mode must be 0, 1 or 2");
+    g_guard_mode.store(mode);
+    return DWCU_SUCCESS;
+}
+
+int64_t dwcu_debug_guard_violations(void) { return g_guard_violations.load(); }
 
 int dwcu_selftest_bounded_wait(int32_t device, int32_t arrive, uint32_t polls)
 {

@@ -379,6 +379,17 @@ int64_t dwcu_launch_count(void);
  * gave up; the device stays usable either way.  No counterpart in the
  * reference, which exits on any device error. */
 int dwcu_selftest_bounded_wait(int32_t device, int32_t arrive, uint32_t polls);
+/* Guard bands, a debugging aid in place of a memory checker: with mode 1,
+ * jobs created afterwards put 4 KB of a fixed pattern before and after
+ * every buffer of their device block, and dwcu_job_destroy compares them
+ * with the pattern; a changed band (a write outside its buffer) is counted
+ * and reported on stderr.  Mode 2 also overwrites one byte of each job's
+ * first band from the host, to check the check.  Mode 0 (the default) adds
+ * nothing.  No counterpart in the reference (which relies on AddressSanitizer
+ * builds of its host code). */
+int dwcu_debug_guards(int32_t mode);
+/* Changed guard bands found so far (all jobs, all threads). */
+int64_t dwcu_debug_guard_violations(void);
 
 #ifdef __cplusplus
 }
