@@ -129,7 +129,7 @@ EXPORTS = [
     "dwcu_tune_set_mode", "dwcu_tune_get_mode", "dwcu_tune_select", "dwcu_tune_plan_count",
     "dwcu_tune_plan_info", "dwcu_tune_force", "dwcu_tune_run", "dwcu_tune_query", "dwcu_tune_clear",
     "dwcu_tune_export", "dwcu_tune_import", "dwcu_psf_prepare_device", "dwcu_selftest_bounded_wait",
-    "dwcu_debug_guards", "dwcu_debug_guard_violations",
+    "dwcu_debug_guards", "dwcu_debug_guard_violations", "dwcu_deconvolve_slabs", "dwcu_slab_layout",
 ]
 
 # pass kinds of the autotuner (dwcu.h)
@@ -158,6 +158,10 @@ def lib() -> ctypes.CDLL:
     L.dwcu_deconvolve_device.restype = ctypes.c_int
     L.dwcu_plan_size.argtypes = [i64, i64, i64, i64, i64, i64, i32, i32, ctypes.POINTER(i64), ctypes.POINTER(i64)]
     L.dwcu_plan_size.restype = ctypes.c_int
+    L.dwcu_deconvolve_slabs.argtypes = [vp, i64, i64, i64, vp, i64, i64, i64, P_opts, i32, vp, vp]
+    L.dwcu_deconvolve_slabs.restype = ctypes.c_int
+    L.dwcu_slab_layout.argtypes = [i64, i64, i64, i64, i64, i64, i32, i32, i32, ctypes.POINTER(i64)]
+    L.dwcu_slab_layout.restype = ctypes.c_int
     L.dwcu_release_cache.argtypes = [i32]
     L.dwcu_release_cache.restype = ctypes.c_int
     L.dwcu_job_create.argtypes = [i64, i64, i64, i64, i64, i64, P_opts, ctypes.POINTER(vp)]
@@ -307,6 +311,43 @@ def run_method(im: np.ndarray, psf: np.ndarray, out: np.ndarray | None = None, *
     _check(lib().dwcu_deconvolve(im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP,
                                  ctypes.byref(o), out.ctypes.data))
     return Result(out, trace[: o.iterations_done].copy(), o)
+
+
+def run_slabs(im: np.ndarray, psf: np.ndarray, parts: int = 2, devices=None, out: np.ndarray | None = None,
+              **kw) -> Result:
+    """:func:`run_method` with the job split over ``parts`` slabs of z planes
+    (dwcu_deconvolve_slabs): one image over several GPUs.  ``devices``: the
+    GPU of each part (default: every part on the ``device`` option)."""
+    im = np.ascontiguousarray(im, dtype=np.float32)
+    psf = np.ascontiguousarray(psf, dtype=np.float32)
+    if im.ndim != 3 or psf.ndim != 3:
+        raise ValueError("image and PSF must be 3-D (P, N, M) arrays")
+    o = make_opts(**kw)
+    cap = max(o.n_iter, o.maxiter, 1)
+    trace = np.zeros(cap, dtype=np.float32)
+    o.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    o.trace_capacity = cap
+    out = _out_array(out, im.shape)
+    dev = None
+    if devices is not None:
+        if len(devices) != parts:
+            raise ValueError("one device per part")
+        dev = (ctypes.c_int32 * parts)(*devices)
+    P, N, M = im.shape
+    pP, pN, pM = psf.shape
+    _check(lib().dwcu_deconvolve_slabs(im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP, ctypes.byref(o),
+                                       parts, dev, out.ctypes.data))
+    return Result(out, trace[: o.iterations_done].copy(), o)
+
+
+def slab_layout(shape, psf_shape, parts: int, part: int, border_quality: int = 2) -> dict:
+    """The planes and z-pass columns of one part of a split job (dwcu_slab_layout)."""
+    P, N, M = shape
+    pP, pN, pM = psf_shape
+    info = (ctypes.c_int64 * 6)()
+    _check(lib().dwcu_slab_layout(M, N, P, pM, pN, pP, border_quality, parts, part, info))
+    keys = ("planes", "image_planes", "col0", "cols", "plane_cols", "Z")
+    return dict(zip(keys, list(info)))
 
 
 def release_cache(device: int = -1) -> None:

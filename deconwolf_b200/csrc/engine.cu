@@ -559,6 +559,11 @@ struct dwcu_job {
     cudaGraphExec_t graph = nullptr; // a graph owned by this job (holding timing events)
     double enqueue_s = 0;          // host time inside job_step
     std::vector<size_t> guards;    // offsets of the guard bands in the block (debug mode)
+    // a part of an image split over GPUs by z planes: the OTF of the part's
+    // z-pass columns (all Z planes) takes the place of the spectrum-sized
+    // OTF, and T holds the columns being transformed
+    long long slab_elems = 0;      // complex elements of each column buffer (0: a whole job)
+    float2 *T = nullptr;
 };
 
 namespace dwcu {
@@ -841,7 +846,9 @@ static int alloc_job(dwcu_job *j)
         off += align256(b);
         return o;
     };
-    size_t o_g = take(G), o_S = take(C), o_K = take(C), o_xa = take(R), o_xb = take(R);
+    const size_t CK = j->slab_elems ? sizeof(float2) * (size_t) j->slab_elems : C;
+    size_t o_g = take(G), o_S = take(C), o_K = take(CK), o_xa = take(R), o_xb = take(R);
+    size_t o_T = j->slab_elems ? take(CK) : 0;
     size_t o_W = need_w ? take(R) : 0;
     size_t o_part = take(sizeof(double) * (size_t) j->nxb);
     size_t o_sc = take(sizeof(JobScalars));
@@ -863,6 +870,7 @@ static int alloc_job(dwcu_job *j)
     j->gimg = (float *) (b + o_g);
     j->S = (float2 *) (b + o_S);
     j->K = (float2 *) (b + o_K);
+    j->T = j->slab_elems ? (float2 *) (b + o_T) : nullptr;
     j->xa = (float *) (b + o_xa);
     j->xb = (float *) (b + o_xb);
     j->W = need_w ? (float *) (b + o_W) : nullptr;
@@ -2073,3 +2081,6 @@ int dwcu_fft_c2r(const float *d_in, int64_t M, int64_t N, int64_t P, float *d_ou
 }
 
 }  // extern "C"
+
+// one image over several GPUs (slabs of z planes)
+#include "slab.cuh"

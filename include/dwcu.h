@@ -112,6 +112,26 @@ int dwcu_deconvolve_device(const float *d_im, int64_t M, int64_t N, int64_t P,
 int dwcu_plan_size(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP,
                    int32_t border_quality, int32_t method, int64_t work[3], int64_t *device_bytes);
 
+/* One image over several GPUs: the dw_function call (as dwcu_deconvolve) with
+ * the job split into nparts slabs of z planes, part p holding the planes
+ * z = l*nparts + p.  Each part runs the x and y passes of its planes on its
+ * GPU; the z pass runs per part on a slab of spectrum columns, gathered from
+ * and scattered back to every part by pitched peer copies (NVLink between
+ * GPUs).  devices[p] is part p's GPU (NULL: every part on s->device; parts may
+ * share a GPU).  For jobs larger than one GPU's memory, where deconwolf tiles
+ * the image (src/dw.c:2001-2229).  Not supported (DWCU_ERROR_UNSUPPORTED):
+ * the low-pass start, and sizes that need periodic margins
+ * (border_quality 0 / 1 without an exact-size transform). */
+int dwcu_deconvolve_slabs(const float *im, int64_t M, int64_t N, int64_t P,
+                          const float *psf, int64_t pM, int64_t pN, int64_t pP,
+                          dwcu_opts *s, int32_t nparts, const int32_t *devices, float *out);
+
+/* The share of part `part` of nparts (host arithmetic, no device):
+ * info[0] z planes, info[1] image planes, info[2] first z-pass column,
+ * info[3] z-pass columns, info[4] columns per plane, info[5] padded Z. */
+int dwcu_slab_layout(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP,
+                     int32_t border_quality, int32_t nparts, int32_t part, int64_t info[6]);
+
 /* ---------------------------------------------------------------- jobs */
 
 /* A job keeps its image, OTF, weights and estimates resident on the device

@@ -73,7 +73,7 @@ def test_no_job_writes_outside_its_buffers():
             g = dw.run_method(im, psf, **kw)
             np.testing.assert_array_equal(g.out, ref.out)
             np.testing.assert_array_equal(g.trace, ref.trace)
-        # tiles, a batch and the server
+        # tiles, a batch, the server and a split job
         im, psf = _inputs((8, 70, 64), (7, 9, 9), 53)
         pp = dw.psf_prepare(psf, im.shape)
         dw.deconvolve_tiled(im, pp, 30, 6, method="shb", n_iter=6)
@@ -91,6 +91,10 @@ def test_no_job_writes_outside_its_buffers():
         for i in ids:
             sv.wait(i)
         sv.close()
+        # one image split into parts (including parts without image planes)
+        for parts in (3, 7):
+            dw.run_slabs(im, psf, parts=parts, method="shb", n_iter=5)
+        dw.run_slabs(im, psf, parts=4, method="rl", n_iter=5)
         assert _violations() == v0
     finally:
         dw.lib().dwcu_debug_guards(0)
