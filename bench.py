@@ -484,6 +484,59 @@ def run_serve(args):
 
 # ---------------------------------------------------------------- B200 arm
 
+def run_split(args):
+    """One 2048 x 2048 x 60 image split into --parts slabs of z planes
+    (dwcu_deconvolve_slabs), parts dealt round-robin over the visible GPUs,
+    beside the whole job on one GPU (dwcu_deconvolve).  With one GPU every
+    part shares it, and the difference is the cost of the split itself (the
+    column transposes run as copies within one GPU's memory)."""
+    import torch
+    import deconwolf_b200 as dw
+    from deconwolf_b200 import synthetic
+    im, psf = synthetic.config_inputs(WORKLOAD, CACHE)
+    ngpu = max(1, torch.cuda.device_count())
+    parts = args.parts
+    devices = [p % ngpu for p in range(parts)]
+    im = _pinned(im)
+    outs = [_pinned(shape=im.shape), _pinned(shape=im.shape)]
+
+    def split():
+        return dw.run_slabs(im, psf, parts=parts, devices=devices, method="shb", n_iter=ITERS, out=outs[0])
+
+    def whole():
+        return dw.run_method(im, psf, method="shb", n_iter=ITERS, out=outs[1])
+
+    for _ in range(args.warmup):
+        split()
+    t = time.perf_counter()
+    loop = []
+    for _ in range(args.steps):
+        res = split()
+        loop.append(res.seconds_iterate)
+    dt = (time.perf_counter() - t) / args.steps
+    whole()
+    t = time.perf_counter()
+    ref = whole()
+    dt_whole = time.perf_counter() - t
+    vox_it = float(im.size) * ITERS
+    P, N, M = im.shape
+    lay = [dw.slab_layout(im.shape, psf.shape, parts, p) for p in range(parts)]
+    print(json.dumps(_common_line(
+        f"Mvoxel*iter/s (SHB, {M}x{N}x{P} split into {parts} parts)", vox_it / dt / 1e6, args,
+        {"workload": "split-2048x2048x60", "image": [M, N, P], "psf": list(psf.shape[::-1]), "parts": parts,
+         "devices": devices, "iterations": ITERS, "method": "shb",
+         "planes_per_part": [q["planes"] for q in lay], "columns_per_part": [q["cols"] for q in lay],
+         "host_buffers": "page-locked image and result"},
+        {"n_gpus": len(set(devices)), "ms_per_step": dt * 1e3,
+         "loop_ms": statistics.median(loop) * 1e3,
+         "whole_job": {"value": vox_it / dt_whole / 1e6, "ms_per_step": dt_whole * 1e3,
+                       "loop_ms": ref.seconds_iterate * 1e3, "how": "dwcu_deconvolve on GPU 0"},
+         "rel_l2_vs_whole": float(np.linalg.norm(res.out.astype(np.float64) - ref.out)
+                                  / np.linalg.norm(ref.out.astype(np.float64))),
+         "iterations_equal": bool(res.iterations == ref.iterations)})), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -493,7 +546,9 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=[WORKLOAD, SMALL, PROFILE_CASE, "shb-2048x256x20", "shb-256x2048x20", "shb-256x256x60",
                              "shb-1124x1124x60",
-                             "tiles-4096x4096x60", "channels-6", "serve-stream", "batch-classes"])
+                             "tiles-4096x4096x60", "channels-6", "serve-stream", "batch-classes",
+                             "split-2048x2048x60"])
+    ap.add_argument("--parts", type=int, default=2, help="split-2048x2048x60: slabs of z planes")
     ap.add_argument("--tilesize", type=int, default=1024)
     ap.add_argument("--requests", type=int, default=60, help="serve-stream: number of requests (full stream: 500)")
     ap.add_argument("--hbm-budget", type=float, default=160e9, help="serve-stream: device bytes for admitted jobs")
@@ -515,6 +570,8 @@ def main():
         return run_serve(args)
     if args.workload == "batch-classes":
         return run_classes(args)
+    if args.workload == "split-2048x2048x60":
+        return run_split(args)
 
     import torch
     import torch.distributed as dist
