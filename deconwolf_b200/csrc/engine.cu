@@ -639,7 +639,7 @@ static int pass_z(dwcu_job *j, int mode, float2 *data, long long nin = -1, long 
 }
 
 static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, const float *srcp, float *dst,
-                  double alpha, double alpha_next, long long tiles = -1)
+                  double alpha, double alpha_next, long long tiles = -1, bool field = true)
 {
     const Geometry &g = j->g;
     XArgs a;
@@ -670,8 +670,9 @@ static int pass_x(dwcu_job *j, int op, int r2c, float2 *S, const float *src, con
     a.rl_clamp = 1;
     a.alpha = alpha;
     a.alpha_next = alpha_next;
-    // the OTF is the shifted PSF, not a periodic field: no margins
-    const bool wrap = S != j->K;
+    // the OTF is the shifted PSF, not a periodic field: no margins (`field`
+    // false: the transform of the OTF into another buffer)
+    const bool wrap = field && S != j->K;
     a.wrapx = (wrap && g.wx) ? 1 : 0;
     a.wM = (int) g.wM;
     a.hx = (int) g.hx;

@@ -27,11 +27,12 @@
 // every other part's.  Within one transpose, part p reads and then writes
 // the same region (its columns of every plane), which no other part touches.
 //
-// Supported: SHB and RL, every stopping rule, flat and identity starts, the
-// Bertero weights (border_quality 1 and 2, and 0 where the exact sizes have
-// transforms).  Not supported: the low-pass start (its z smoothing needs
-// whole image columns) and periodic margins (axes without an exact-size
-// transform at border_quality 0 / 1).
+// Supported: SHB and RL, every stopping rule, every start (the low-pass
+// start smooths the whole image on part 0's GPU and deals its planes out),
+// every border quality, and periodic margins along x and y (rows within a
+// part's planes).  Not supported: periodic margins along z (a z length
+// without an exact-size transform at border_quality 0 / 1: the margin planes
+// would be copies of other parts' planes).
 
 struct dwcu_slab;
 
@@ -189,13 +190,10 @@ static int slab_create(long long M, long long N, long long P, long long pM, long
     if (!s) return fail(DWCU_ERROR_INVALID_VALUE, "opts is NULL");
     TRY(check_opts(*s));
     if (nparts < 1 || nparts > 64) return fail(DWCU_ERROR_INVALID_VALUE, "parts must be 1..64 (got %d)", nparts);
-    if (s->start_condition == DWCU_START_LP)
-        return fail(DWCU_ERROR_UNSUPPORTED, "the low-pass start needs whole image columns: not with parts");
     Geometry g;
     TRY(make_geometry(M, N, P, pM, pN, pP, s->border_quality, g));
-    if (g.wx || g.wy || g.wz)
-        return fail(DWCU_ERROR_UNSUPPORTED, "job %lld x %lld x %lld needs periodic margins: not with parts", g.wM,
-                    g.wN, g.wP);
+    if (g.wz)
+        return fail(DWCU_ERROR_UNSUPPORTED, "job z size %lld needs periodic margins along z: not with parts", g.wP);
     if (nparts > g.Z) return fail(DWCU_ERROR_UNSUPPORTED, "%d parts for %lld z planes", nparts, g.Z);
     if (g.NKB * g.Y < nparts) return fail(DWCU_ERROR_UNSUPPORTED, "too few z-pass columns for %d parts", nparts);
     const int dev0 = devices ? devices[0] : s->device;
@@ -321,6 +319,72 @@ static int slab_conv(dwcu_slab *sl, int conj, bool in_img, bool out_img)
     return DWCU_SUCCESS;
 }
 
+// The low-pass start (method_shb.c:278-285, method_rl.c:290-297): the image
+// smoothed by fim_gsmooth (sigma 8) along x, y and z -- the z smoothing
+// needs whole image columns, so the whole image is smoothed on part 0's GPU
+// (job_setup's kernels and taps) -- then each part's image planes are copied
+// into the corner of its zeroed x_0.
+static int slab_lowpass_start(dwcu_slab *sl, const float *im)
+{
+    if (sl->s.start_condition != DWCU_START_LP) return DWCU_SUCCESS;
+    const Geometry &g = sl->g;
+    const int n = (int) sl->parts.size();
+    SlabPart &p0 = sl->parts[0];
+    CU(cudaSetDevice(p0.device));
+    const long long nimg = g.M * g.N * g.P;
+    float *t = nullptr;
+    CU(cudaMalloc(&t, sizeof(float) * (size_t) (2 * nimg)));
+    float *t1 = t, *t2 = t + nimg;
+    int rc = DWCU_SUCCESS;
+    auto run = [&]() -> int {
+        cudaStream_t st = p0.stream;
+        const int gb = (int) std::min<long long>(148 * 16, (nimg + 255) / 256);
+        GaussTaps K = gauss_taps(8.0f);
+        CU(cudaMemcpyAsync(t2, im, sizeof(float) * (size_t) nimg, cudaMemcpyHostToDevice, st));
+        k_gsmooth_axis<<<gb, 256, 0, st>>>(t2, t1, (int) g.M, (int) g.N, (int) g.P, 0, K);
+        CHECK_LAUNCH();
+        k_gsmooth_axis<<<gb, 256, 0, st>>>(t1, t2, (int) g.M, (int) g.N, (int) g.P, 1, K);
+        CHECK_LAUNCH();
+        const float *lp = t2;
+        if (g.P > 1) {
+            // fim_gsmooth_aniso trims the z kernel to at most 2P-1 taps
+            GaussTaps Kz = K;
+            int off = 0;
+            while (Kz.n > 2 * g.P - 1) {
+                ++off;
+                Kz.n -= 2;
+            }
+            for (int i = 0; i < Kz.n; ++i) Kz.k[i] = K.k[i + off];
+            k_gsmooth_axis<<<gb, 256, 0, st>>>(t2, t1, (int) g.M, (int) g.N, (int) g.P, 2, Kz);
+            CHECK_LAUNCH();
+            lp = t1;
+        }
+        CU(cudaEventRecord(p0.ev, st));
+        for (int p = 0; p < n; ++p) {
+            SlabPart &pt = sl->parts[(size_t) p];
+            dwcu_job *j = pt.j;
+            CU(cudaSetDevice(pt.device));
+            if (p > 0) CU(cudaStreamWaitEvent(pt.stream, p0.ev, 0));
+            CU(cudaMemsetAsync(j->xa, 0, sizeof(float) * (size_t) j->g.real_elems(), pt.stream));
+            for (long long l = 0; l < pt.pl; ++l) {
+                const long long z = l * n + p;
+                CU(cudaMemcpy2DAsync(j->xa + l * g.Y * g.XP, sizeof(float) * g.XP, lp + z * g.M * g.N,
+                                     sizeof(float) * g.M, sizeof(float) * g.M, g.N, cudaMemcpyDefault, pt.stream));
+            }
+        }
+        return DWCU_SUCCESS;
+    };
+    rc = run();
+    // the work space is freed once every part's copies are done
+    for (auto &pt : sl->parts) {
+        cudaSetDevice(pt.device);
+        cudaStreamSynchronize(pt.stream);
+    }
+    cudaSetDevice(p0.device);
+    cudaFree(t);
+    return rc;
+}
+
 // image planes and PSF into the parts; statistics, OTF, weights and the start
 // estimate (job_setup's steps, method_shb.c:108-296, over the parts)
 static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
@@ -376,6 +440,20 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
     }
     if (flags & 1) return fail(DWCU_ERROR_INPUT, "the image contains non-finite values");
     if (flags & 2) return fail(DWCU_ERROR_INPUT, "the PSF contains non-finite values");
+    if (g.wx || g.wy) {
+        // the periodic margins assume the PSF maximum within h of both ends (as job_setup)
+        long long am = 0;
+        SlabPart &p0 = sl->parts[0];
+        CU(cudaSetDevice(p0.device));
+        CU(cudaMemcpy(&am, p0.j->amax, sizeof am, cudaMemcpyDeviceToHost));
+        const long long ax = am % g.pM, ay = (am / g.pM) % g.pN;
+        auto off = [](long long a, long long p) { return std::max(a, p - 1 - a); };
+        if ((g.wx && off(ax, g.pM) > g.hx) || (g.wy && off(ay, g.pN) > g.hy))
+            return fail(DWCU_ERROR_UNSUPPORTED,
+                        "border_quality %d with a job size that has no exact transform needs the PSF maximum at "
+                        "its centre (maximum at %lld, %lld of %lld x %lld)",
+                        sl->s.border_quality, ax, ay, g.pM, g.pN);
+    }
     JobScalars all{};
     all.gmin = gmin;
     all.sumg = sumg;
@@ -398,7 +476,7 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
             j->psf_dev, (int) g.pM, (int) g.pN, (int) g.pP, j->amax, j->xb, (int) g.X, (int) g.Y, (int) g.Z,
             (int) g.XP, scale, n, p);
         CHECK_LAUNCH();
-        TRY(pass_x(j, XOP_FWD_COPY, 1, j->S, j->xb, nullptr, nullptr, 0, 0));
+        TRY(pass_x(j, XOP_FWD_COPY, 1, j->S, j->xb, nullptr, nullptr, 0, 0, -1, false));
         TRY(pass_y(j, LINES_FWD, j->S));
     }
     // ... and the z transform of the part's columns, kept as its OTF
@@ -422,6 +500,7 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
         }
     }
     // start estimate (method_shb.c:264-276); x_{-1} = x_0
+    TRY(slab_lowpass_start(sl, im));
     for (auto &pt : sl->parts) {
         dwcu_job *j = pt.j;
         CU(cudaSetDevice(pt.device));
@@ -432,7 +511,7 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
         if (sl->s.start_condition == DWCU_START_FLAT) {
             k_fill_scalar<<<fb, 256, 0, st>>>(j->xa, nv, j->sc);
             CHECK_LAUNCH();
-        } else {
+        } else if (sl->s.start_condition == DWCU_START_IDENTITY) {
             CU(cudaMemsetAsync(j->xa, 0, R, st));
             if (pt.pl > 0) {
                 k_embed_image<<<fb, 256, 0, st>>>(j->gimg, g.GP, (int) g.M, (int) g.N, (int) pt.pl, j->xa, (int) g.XP,

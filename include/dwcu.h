@@ -120,8 +120,8 @@ int dwcu_plan_size(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int6
  * GPUs).  devices[p] is part p's GPU (NULL: every part on s->device; parts may
  * share a GPU).  For jobs larger than one GPU's memory, where deconwolf tiles
  * the image (src/dw.c:2001-2229).  Not supported (DWCU_ERROR_UNSUPPORTED):
- * the low-pass start, and sizes that need periodic margins
- * (border_quality 0 / 1 without an exact-size transform). */
+ * a job z size that needs periodic margins (border_quality 0 / 1 without an
+ * exact-size z transform). */
 int dwcu_deconvolve_slabs(const float *im, int64_t M, int64_t N, int64_t P,
                           const float *psf, int64_t pM, int64_t pN, int64_t pP,
                           dwcu_opts *s, int32_t nparts, const int32_t *devices, float *out);

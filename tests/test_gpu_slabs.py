@@ -61,6 +61,12 @@ CASES = [
     (dict(method="shb", n_iter=10, border_quality=1), (9, 20, 19), (5, 7, 9)),
     (dict(method="rl", n_iter=10, border_quality=0), (10, 24, 20), (5, 7, 9)),
     (dict(method="shb", n_iter=8, bg=3.0, positivity=False), (9, 22, 19), (5, 7, 9)),
+    (dict(method="shb", n_iter=7, start=po.START_LP), (9, 22, 19), (5, 7, 9)),
+    (dict(method="rl", n_iter=7, start=po.START_LP), (20, 64, 70), (9, 11, 13)),
+    # periodic margins along y (job 24 x 32 x 12), along x (30 x 24 x 12), both (bq 0, 30 x 32 x 10)
+    (dict(method="shb", n_iter=10, border_quality=1), (9, 22, 19), (5, 7, 9)),
+    (dict(method="rl", n_iter=10, border_quality=1), (9, 20, 17), (5, 7, 9)),
+    (dict(method="shb", n_iter=10, border_quality=0), (10, 26, 22), (5, 7, 9)),
 ]
 
 
@@ -104,10 +110,13 @@ def test_parts_match_the_oracle(method):
 
 
 def test_unsupported_splits_are_refused():
-    im, psf = _inputs()
+    # periodic margins along z (job z size 13 at bq 1: transformed at 20)
+    im, psf = _inputs((9, 22, 19), (7, 7, 9))
+    assert dw.plan_size(im.shape, psf.shape, border_quality=1)[0][2] == 20
     with pytest.raises(dw.DwcuError) as e:
-        dw.run_slabs(im, psf, parts=2, method="shb", n_iter=4, start=po.START_LP)
+        dw.run_slabs(im, psf, parts=2, method="shb", n_iter=4, border_quality=1)
     assert e.value.code == ERROR_UNSUPPORTED
+    im, psf = _inputs()
     Z = dw.plan_size(im.shape, psf.shape)[0][2]
     with pytest.raises(dw.DwcuError) as e:
         dw.run_slabs(im, psf, parts=Z + 1, method="shb", n_iter=4)
