@@ -525,6 +525,7 @@ def run_split(args):
         f"Mvoxel*iter/s (SHB, {M}x{N}x{P} split into {parts} parts)", vox_it / dt / 1e6, args,
         {"workload": "split-2048x2048x60", "image": [M, N, P], "psf": list(psf.shape[::-1]), "parts": parts,
          "devices": devices, "iterations": ITERS, "method": "shb",
+         "exchange": "gathered copies" if os.environ.get("DWCU_SLAB_TRANSPOSE") == "copy" else "in place (plane table)",
          "planes_per_part": [q["planes"] for q in lay], "columns_per_part": [q["cols"] for q in lay],
          "host_buffers": "page-locked image and result"},
         {"n_gpus": len(set(devices)), "ms_per_step": dt * 1e3,

@@ -563,6 +563,7 @@ struct dwcu_job {
     // z-pass columns (all Z planes) takes the place of the spectrum-sized
     // OTF, and T holds the columns being transformed
     long long slab_elems = 0;      // complex elements of each column buffer (0: a whole job)
+    bool slab_copies = false;      // the z pass works on gathered copies (T allocated)
     float2 *T = nullptr;
 };
 
@@ -574,7 +575,8 @@ static int trace_cap(const dwcu_opts &s) { return std::max(1, std::max(s.n_iter,
 
 static int launch_lines(dwcu_job *j, const LinesPlan *p, const float2 *tw, long long n, long long line_stride,
                         long long outer_stride, long long nouter, long long ncols, int mode, float2 *data,
-                        const char *axis, long long nin = -1, long long nout = -1)
+                        const char *axis, long long nin = -1, long long nout = -1, float2 *const *planes = nullptr,
+                        long long col0 = 0)
 {
     if (nin < 0) nin = n;
     if (nout < 0) nout = n;
@@ -590,6 +592,8 @@ static int launch_lines(dwcu_job *j, const LinesPlan *p, const float2 *tw, long 
     a.mode = mode;
     a.nin = (int) nin;
     a.nout = (int) nout;
+    a.planes = planes;
+    a.col0 = col0;
     long long nb = (long long) a.ntiles * nouter;
     if (nb > 0x7fffffffLL) return fail(DWCU_ERROR_UNSUPPORTED, "grid too large");
     static const char *names[] = {"lines_fwd", "lines_inv", "lines_conv", "lines_conv_conj"};
@@ -849,7 +853,7 @@ static int alloc_job(dwcu_job *j)
     };
     const size_t CK = j->slab_elems ? sizeof(float2) * (size_t) j->slab_elems : C;
     size_t o_g = take(G), o_S = take(C), o_K = take(CK), o_xa = take(R), o_xb = take(R);
-    size_t o_T = j->slab_elems ? take(CK) : 0;
+    size_t o_T = (j->slab_elems && j->slab_copies) ? take(CK) : 0;
     size_t o_W = need_w ? take(R) : 0;
     size_t o_part = take(sizeof(double) * (size_t) j->nxb);
     size_t o_sc = take(sizeof(JobScalars));
@@ -871,7 +875,7 @@ static int alloc_job(dwcu_job *j)
     j->gimg = (float *) (b + o_g);
     j->S = (float2 *) (b + o_S);
     j->K = (float2 *) (b + o_K);
-    j->T = j->slab_elems ? (float2 *) (b + o_T) : nullptr;
+    j->T = (j->slab_elems && j->slab_copies) ? (float2 *) (b + o_T) : nullptr;
     j->xa = (float *) (b + o_xa);
     j->xb = (float *) (b + o_xb);
     j->W = need_w ? (float *) (b + o_W) : nullptr;

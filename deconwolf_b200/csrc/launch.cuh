@@ -48,12 +48,17 @@ inline int persistent_grid(KernelOnce &ko, K kernel, int threads, size_t smem, i
 template <class RD, int T>
 void launch_lines_t(const LinesArgs &a, int nblocks, cudaStream_t st)
 {
-    static KernelOnce ko;
+    static KernelOnce ko, kp;
     using C = LinesCfg<RD, T>;
-    ensure_smem(ko, k_lines<RD, T>, C::SMEM_BYTES);
     constexpr int tpl = C::THREADS / T;
     const size_t smem = a.mode >= LINES_CONV ? C::SMEM_BYTES : C::SMEM_FFT;
-    k_lines<RD, T><<<nblocks, dim3(T, tpl), smem, st>>>(a);
+    if (a.planes) {
+        ensure_smem(kp, k_lines<RD, T, true>, C::SMEM_BYTES);
+        k_lines<RD, T, true><<<nblocks, dim3(T, tpl), smem, st>>>(a);
+    } else {
+        ensure_smem(ko, k_lines<RD, T>, C::SMEM_BYTES);
+        k_lines<RD, T><<<nblocks, dim3(T, tpl), smem, st>>>(a);
+    }
 }
 
 template <class RD, int DIR>

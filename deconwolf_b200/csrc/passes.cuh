@@ -218,6 +218,11 @@ struct LinesArgs {
     int mode;
     int nin;                 // elements [0, nin) of a line are read; the rest are zero
     int nout;                // elements [0, nout) of a line are written
+    // planes mode (a job split by z planes over GPUs): element n of column c
+    // is planes[n][col0 + c], plane n on whichever GPU holds it (peer
+    // loads and stores); `data` is unused and `line_stride` is the OTF's
+    float2 *const *planes = nullptr;
+    long long col0 = 0;
 };
 
 template <class RD, int T>
@@ -234,7 +239,7 @@ struct LinesCfg {
         : (THREADS * 2 <= 1024 && SMEM_BYTES * 2 <= 225 * 1024) ? 2 : 1;
 };
 
-template <class RD, int T>
+template <class RD, int T, bool PL = false>
 __global__ void __launch_bounds__(LinesCfg<RD, T>::THREADS, LinesCfg<RD, T>::MIN_BLOCKS)
 k_lines(LinesArgs a)
 {
@@ -250,6 +255,13 @@ k_lines(LinesArgs a)
     const long long off = outer * a.outer_stride + col;
     float2 *base = a.data + off;
     const long long ls = a.line_stride;
+    // element n of this thread's line
+    auto elem = [&](int n) -> float2 * {
+        if constexpr (PL)
+            return a.planes[n] + (a.col0 + col);
+        else
+            return base + (long long) n * ls;
+    };
     const int mode = a.mode;
     auto smem = [&](int, int i) { return sm + (size_t) i * T + line; };
     using Cfg = LinesCfg<RD, T>;
@@ -273,7 +285,7 @@ k_lines(LinesArgs a)
 #pragma unroll
         for (int r = 0; r < RD::RA; ++r) {
             const int n = t + r * (N / RD::RA);
-            v[0][r] = (valid && n < a.nin) ? base[(long long) n * ls] : make_float2(0.f, 0.f);
+            v[0][r] = (valid && n < a.nin) ? *elem(n) : make_float2(0.f, 0.f);
         }
     }
     float2 o[1][RD::RL];
@@ -286,7 +298,7 @@ k_lines(LinesArgs a)
         if (t < SL && valid) {
 #pragma unroll
             for (int r = 0; r < RD::RL; ++r)
-                if (t + r * SL < a.nout) base[(long long) (t + r * SL) * ls] = o[0][r];
+                if (t + r * SL < a.nout) *elem(t + r * SL) = o[0][r];
         }
         return;
     }
@@ -316,7 +328,7 @@ k_lines(LinesArgs a)
     if (t < SQ && valid) {
 #pragma unroll
         for (int r = 0; r < RV::RL; ++r)
-            if (t + r * SQ < a.nout) base[(long long) (t + r * SQ) * ls] = q[0][r];
+            if (t + r * SQ < a.nout) *elem(t + r * SQ) = q[0][r];
     }
 }
 

@@ -13,13 +13,17 @@
 // same share of the image planes (the pruned passes stay balanced).  The x
 // and y passes need nothing from other parts.  The z pass needs whole z
 // lines: part p transforms the columns [c0, c0 + nc) of every plane (a
-// plane's NKB*Y*KB complex elements, nc a multiple of KB), gathered into its
+// plane's NKB*Y*KB complex elements, nc a multiple of KB).  Where every pair
+// of the parts' GPUs has peer access (always, for parts on one GPU), the z
+// pass reads and writes those columns where they lie, through a table of
+// the Z planes' addresses (k_lines' planes mode: one kernel does the
+// transform and the exchange, the NVLink transfer overlapping the FFT
+// arithmetic block by block).  Otherwise the columns are gathered into a
 // column buffer T ([Z][nc], plane z at z*nc) by one pitched copy from each
-// part (part q's planes are the rows q, q+n, ... of T) and scattered back
-// the same way after the transform.  Between GPUs the copies run on the
-// copy engines over NVLink (peer access) and land in local HBM before any
-// kernel reads them; parts on one GPU copy within its memory.  The OTF of the
-// part's columns stays with the part ([Z][nc]).
+// part (part q's planes are the rows q, q+n, ... of T), transformed there,
+// and scattered back the same way (copy engines; staged through the host
+// where the GPUs have no peer access).  The OTF of the part's columns stays
+// with the part ([Z][nc]).
 //
 // Order between parts (slab_barrier): before a gather, every part's writes of
 // the planes it gathers are complete; before the y pass after a scatter,
@@ -46,6 +50,7 @@ struct SlabPart {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;      // ordering between parts
     double *psum = nullptr;        // per iteration: the error sum of the part's tiles
+    float2 **planes = nullptr;     // planes mode: the address of every plane z (on this part's GPU)
 };
 
 // the planes and z-pass columns of part p of n (host arithmetic only)
@@ -114,6 +119,7 @@ struct dwcu_slab {
     dwcu::Geometry g;              // the whole job
     std::vector<dwcu::SlabPart> parts;
     double *sums = nullptr;        // on part 0's device: the parts' error sums of one iteration
+    bool copies = false;           // z pass on gathered copies instead of in place
     dwcu::Iter it;
     int k_next = -1;
     bool spectrum_ready = false;
@@ -137,6 +143,7 @@ static void slab_destroy(dwcu_slab *sl)
         cudaSetDevice(pt.device);
         if (pt.j) dwcu_job_destroy(pt.j);
         if (pt.psum) cudaFree(pt.psum);
+        if (pt.planes) cudaFree(pt.planes);
         if (pt.ev) cudaEventDestroy(pt.ev);
         if (pt.stream) cudaStreamDestroy(pt.stream);
     }
@@ -171,6 +178,7 @@ static int slab_part_create(dwcu_slab *sl, int p, int device)
     j->ctx = ctx;
     j->stream = pt.stream;
     j->slab_elems = g.Z * pt.nc;
+    j->slab_copies = sl->copies;
     TRY(alloc_job(j));
     TRY(get_twiddles(ctx, g.X, &j->tw_x));
     TRY(get_twiddles(ctx, g.X / 2, &j->tw_l));
@@ -205,6 +213,17 @@ static int slab_create(long long M, long long N, long long P, long long pM, long
     sl->s = *s;
     sl->g = g;
     sl->parts.resize((size_t) nparts);
+    // the z pass in place needs peer access between every pair of the parts'
+    // GPUs; DWCU_SLAB_TRANSPOSE=copy asks for the copies regardless
+    const char *tr = getenv("DWCU_SLAB_TRANSPOSE");
+    sl->copies = tr && strcmp(tr, "copy") == 0;
+    for (int p = 0; p < nparts; ++p)
+        for (int q = 0; q < nparts; ++q) {
+            const int a = devices ? devices[p] : s->device, b = devices ? devices[q] : s->device;
+            int can = 0;
+            if (a != b && (cudaDeviceCanAccessPeer(&can, a, b) != cudaSuccess || !can)) sl->copies = true;
+        }
+    cudaGetLastError();
     int rc = DWCU_SUCCESS;
     for (int p = 0; p < nparts && rc == DWCU_SUCCESS; ++p) rc = slab_part_create(sl, p, devices ? devices[p] : s->device);
     // peer access between the parts' GPUs, where the devices allow it (the
@@ -219,6 +238,19 @@ static int slab_create(long long M, long long N, long long P, long long pM, long
             if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) rc = fail(DWCU_ERROR_CUDA, "peer access %d -> %d: %s", a, b, cudaGetErrorString(e));
             cudaGetLastError();
         }
+    // planes mode: every part's table of the Z planes' addresses
+    if (rc == DWCU_SUCCESS && !sl->copies) {
+        const long long plane = g.NKB * g.Y * KB;
+        std::vector<float2 *> tab((size_t) g.Z);
+        for (long long z = 0; z < g.Z; ++z) tab[(size_t) z] = sl->parts[(size_t) (z % nparts)].j->S + (z / nparts) * plane;
+        for (auto &pt : sl->parts) {
+            if (rc != DWCU_SUCCESS) break;
+            cudaSetDevice(pt.device);
+            if (cudaMalloc(&pt.planes, sizeof(float2 *) * (size_t) g.Z) != cudaSuccess ||
+                cudaMemcpy(pt.planes, tab.data(), sizeof(float2 *) * (size_t) g.Z, cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = fail(DWCU_ERROR_OUT_OF_MEMORY, "the plane table could not be set up");
+        }
+    }
     if (rc == DWCU_SUCCESS) {
         cudaSetDevice(dev0);
         if (cudaMalloc(&sl->sums, sizeof(double) * (size_t) nparts) != cudaSuccess)
@@ -305,10 +337,17 @@ static int slab_conv(dwcu_slab *sl, int conj, bool in_img, bool out_img)
         if (h > 0) TRY(pass_y(pt.j, LINES_FWD, pt.j->S, h));
     }
     TRY(slab_barrier(sl));
+    const int mode = conj ? LINES_CONV_CONJ : LINES_CONV;
     for (auto &pt : sl->parts) {
-        TRY(slab_transpose(sl, pt, pt.j->T, in_img, false));
-        TRY(slab_zpass(sl, pt, conj ? LINES_CONV_CONJ : LINES_CONV, pt.j->T, in_img ? g.P : g.Z, out_img ? g.P : g.Z));
-        TRY(slab_transpose(sl, pt, pt.j->T, out_img, true));
+        if (sl->copies) {
+            TRY(slab_transpose(sl, pt, pt.j->T, in_img, false));
+            TRY(slab_zpass(sl, pt, mode, pt.j->T, in_img ? g.P : g.Z, out_img ? g.P : g.Z));
+            TRY(slab_transpose(sl, pt, pt.j->T, out_img, true));
+        } else {
+            CU(cudaSetDevice(pt.device));
+            TRY(launch_lines(pt.j, g.zp, pt.j->tw_z, g.Z, pt.nc, 0, 1, pt.nc, mode, pt.j->K, "z", in_img ? g.P : g.Z,
+                             out_img ? g.P : g.Z, pt.planes, pt.c0));
+        }
     }
     TRY(slab_barrier(sl));
     for (auto &pt : sl->parts) {

@@ -115,9 +115,11 @@ int dwcu_plan_size(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int6
 /* One image over several GPUs: the dw_function call (as dwcu_deconvolve) with
  * the job split into nparts slabs of z planes, part p holding the planes
  * z = l*nparts + p.  Each part runs the x and y passes of its planes on its
- * GPU; the z pass runs per part on a slab of spectrum columns, gathered from
- * and scattered back to every part by pitched peer copies (NVLink between
- * GPUs).  devices[p] is part p's GPU (NULL: every part on s->device; parts may
+ * GPU; the z pass runs per part on a slab of spectrum columns of every
+ * plane, read and written in place over peer access (NVLink) where every
+ * pair of the GPUs has it, else on copies gathered from and scattered back
+ * to every part (environment DWCU_SLAB_TRANSPOSE=copy forces the copies).
+ * devices[p] is part p's GPU (NULL: every part on s->device; parts may
  * share a GPU).  For jobs larger than one GPU's memory, where deconwolf tiles
  * the image (src/dw.c:2001-2229).  Not supported (DWCU_ERROR_UNSUPPORTED):
  * a job z size that needs periodic margins (border_quality 0 / 1 without an

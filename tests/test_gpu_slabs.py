@@ -1,7 +1,9 @@
 """One image split over several GPUs by z planes (dwcu_deconvolve_slabs),
-with every part on one GPU (the parts, their transposes and the ordering
-between them run as they would on several GPUs; only the copies stay in one
-GPU's memory).
+with every part on one GPU (the parts, their exchanges and the ordering
+between them run as they would on several GPUs; only the data stays in one
+GPU's memory).  Both forms of the z pass's exchange run: in place through
+the plane table (the default where the GPUs have peer access) and on
+gathered copies (DWCU_SLAB_TRANSPOSE=copy, the form for GPUs without).
 
 * One part runs the whole job's kernels on the same data: equal to
   dwcu_deconvolve bit for bit.
@@ -27,6 +29,15 @@ SPLIT_TRACE_TOL = 1e-6
 ERROR_UNSUPPORTED = 2
 
 
+@pytest.fixture(params=["direct", "copy"])
+def transpose(request, monkeypatch):
+    if request.param == "copy":
+        monkeypatch.setenv("DWCU_SLAB_TRANSPOSE", "copy")
+    else:
+        monkeypatch.delenv("DWCU_SLAB_TRANSPOSE", raising=False)
+    return request.param
+
+
 def _inputs(shape=(9, 22, 19), psf_shape=(5, 7, 9), seed=7):
     psf = gauss_psf(psf_shape, (1.2, 1.5, 1.7), seed=seed, jitter=0.2)
     im = poisson_image(shape, psf, seed=seed, bg=50.0, npts=15)
@@ -40,7 +51,7 @@ def _trace_err(a, b):
 
 
 @pytest.mark.parametrize("method", ["shb", "rl"])
-def test_one_part_equals_the_whole_job(method):
+def test_one_part_equals_the_whole_job(method, transpose):
     im, psf = _inputs()
     a = dw.run_method(im, psf, method=method, n_iter=12)
     b = dw.run_slabs(im, psf, parts=1, method=method, n_iter=12)
@@ -78,7 +89,7 @@ def _id(v):
 
 @pytest.mark.parametrize("parts", [2, 3, 5])
 @pytest.mark.parametrize("case,shape,psf_shape", CASES, ids=_id)
-def test_parts_match_the_whole_job(case, shape, psf_shape, parts):
+def test_parts_match_the_whole_job(case, shape, psf_shape, parts, transpose):
     im, psf = _inputs(shape, psf_shape)
     a = dw.run_method(im, psf, **case)
     b = dw.run_slabs(im, psf, parts=parts, **case)
@@ -87,7 +98,7 @@ def test_parts_match_the_whole_job(case, shape, psf_shape, parts):
     assert _trace_err(b.trace, a.trace) < SPLIT_TRACE_TOL
 
 
-def test_parts_without_image_planes():
+def test_parts_without_image_planes(transpose):
     # 3 image planes, a 7-plane job: parts 3..6 hold no image plane
     im, psf = _inputs((3, 30, 31), (5, 7, 9))
     assert dw.plan_size(im.shape, psf.shape)[0][2] == 7
@@ -99,7 +110,7 @@ def test_parts_without_image_planes():
 
 
 @pytest.mark.parametrize("method", ["shb", "rl"])
-def test_parts_match_the_oracle(method):
+def test_parts_match_the_oracle(method, transpose):
     im, psf = _inputs((20, 64, 70), (9, 11, 13))
     impl = "reference" if po.available("reference") else "port"
     r = po.deconvolve(im, psf, impl=impl, method=method, n_iter=20)
