@@ -116,6 +116,13 @@ class ServerStats(ctypes.Structure):
                 ("voxel_iterations", ctypes.c_double), ("wall_s", ctypes.c_double)]
 
 
+class JobState(ctypes.Structure):
+    """dwcu_job_state: a job's iteration state between iterations."""
+    _fields_ = [("volume_elems", ctypes.c_int64), ("next_iter", ctypes.c_int32), ("done_iters", ctypes.c_int32),
+                ("iter", ctypes.c_int32), ("error", ctypes.c_float), ("lasterror", ctypes.c_float),
+                ("bg", ctypes.c_float)]
+
+
 # every symbol include/dwcu.h declares
 EXPORTS = [
     "dwcu_opts_init", "dwcu_deconvolve", "dwcu_deconvolve_device", "dwcu_plan_size",
@@ -130,6 +137,7 @@ EXPORTS = [
     "dwcu_tune_plan_info", "dwcu_tune_force", "dwcu_tune_run", "dwcu_tune_query", "dwcu_tune_clear",
     "dwcu_tune_export", "dwcu_tune_import", "dwcu_psf_prepare_device", "dwcu_selftest_bounded_wait",
     "dwcu_debug_guards", "dwcu_debug_guard_violations", "dwcu_deconvolve_slabs", "dwcu_slab_layout",
+    "dwcu_job_snapshot", "dwcu_job_restore",
 ]
 
 # pass kinds of the autotuner (dwcu.h)
@@ -180,6 +188,10 @@ def lib() -> ctypes.CDLL:
     L.dwcu_job_set_stream.restype = ctypes.c_int
     L.dwcu_job_bytes.argtypes = [vp]
     L.dwcu_job_bytes.restype = i64
+    L.dwcu_job_snapshot.argtypes = [vp, vp, vp, vp, i32, ctypes.POINTER(JobState)]
+    L.dwcu_job_snapshot.restype = ctypes.c_int
+    L.dwcu_job_restore.argtypes = [vp, vp, vp, vp, ctypes.POINTER(JobState)]
+    L.dwcu_job_restore.restype = ctypes.c_int
     L.dwcu_last_error.argtypes = []
     L.dwcu_last_error.restype = ctypes.c_char_p
     L.dwcu_abi_version.restype = ctypes.c_int
@@ -603,6 +615,33 @@ class Job:
 
     def nbytes(self) -> int:
         return int(lib().dwcu_job_bytes(self.h))
+
+    def snapshot(self) -> dict:
+        """The job's state between iterations (dwcu_job_snapshot): x_k, x_{k-1}
+        (SHB), the error trace and the stopping rule's counters."""
+        st = JobState()
+        _check(lib().dwcu_job_snapshot(self.h, None, None, None, 0, ctypes.byref(st)))
+        x = np.empty(st.volume_elems, dtype=np.float32)
+        xp = np.empty(st.volume_elems, dtype=np.float32) if self.opts.method == METHOD_SHB else None
+        cap = max(self.opts.n_iter, self.opts.maxiter, 1)
+        trace = np.zeros(cap, dtype=np.float32)
+        _check(lib().dwcu_job_snapshot(self.h, x.ctypes.data, None if xp is None else xp.ctypes.data,
+                                       trace.ctypes.data, cap, ctypes.byref(st)))
+        return dict(x=x, x_prev=xp, trace=trace[: st.done_iters].copy(), next_iter=st.next_iter,
+                    done_iters=st.done_iters, iter=st.iter, error=st.error, lasterror=st.lasterror, bg=st.bg)
+
+    def restore(self, snap: dict) -> None:
+        """Continue from :meth:`snapshot` of a job with the same image, PSF and
+        options (this job set up already): dwcu_job_restore."""
+        st = JobState()
+        st.volume_elems = snap["x"].size
+        for k in ("next_iter", "done_iters", "iter", "error", "lasterror", "bg"):
+            setattr(st, k, snap[k])
+        x = np.ascontiguousarray(snap["x"], dtype=np.float32)
+        xp = None if snap["x_prev"] is None else np.ascontiguousarray(snap["x_prev"], dtype=np.float32)
+        tr = np.ascontiguousarray(snap["trace"], dtype=np.float32)
+        _check(lib().dwcu_job_restore(self.h, x.ctypes.data, None if xp is None else xp.ctypes.data,
+                                      tr.ctypes.data if tr.size else None, ctypes.byref(st)))
 
     def result(self, out=None, on_device: bool = False) -> Result:
         o = Opts()

@@ -1951,6 +1951,68 @@ int dwcu_job_set_stream(dwcu_job *job, void *stream)
 
 int64_t dwcu_job_bytes(const dwcu_job *job) { return job ? (int64_t) job->bytes : 0; }
 
+// Between iterations a job's state is x_k (xa), x_{k-1} (xb, SHB), the error
+// trace and the stopping rule's counters; the spectrum is recomputed from
+// the estimates when the job continues (iter_input), and everything else
+// (image, OTF, weights, scalars) by its set-up.
+int dwcu_job_snapshot(dwcu_job *j, float *x, float *x_prev, float *trace, int32_t trace_capacity,
+                      dwcu_job_state *st)
+{
+    if (!j || !st) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    if (!j->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "snapshot before setup");
+    memset(st, 0, sizeof *st);
+    st->volume_elems = j->g.real_elems();
+    st->next_iter = j->finished ? -1 : j->k_next;
+    st->done_iters = j->done_iters;
+    st->iter = j->it.iter;
+    st->error = j->it.error;
+    st->lasterror = j->it.lasterror;
+    st->bg = j->s.bg;
+    if (!x) return DWCU_SUCCESS;
+    const bool shb = (j->s.method == DWCU_METHOD_SHB);
+    if (shb && !x_prev) return fail(DWCU_ERROR_INVALID_VALUE, "an SHB snapshot needs x_prev");
+    CU(cudaSetDevice(j->s.device));
+    const size_t R = sizeof(float) * (size_t) st->volume_elems;
+    CU(cudaMemcpyAsync(x, j->xa, R, cudaMemcpyDeviceToHost, j->stream));
+    if (shb) CU(cudaMemcpyAsync(x_prev, j->xb, R, cudaMemcpyDeviceToHost, j->stream));
+    const int ne = std::min(j->done_iters, std::max(0, (int) trace_capacity));
+    if (trace && ne > 0) CU(cudaMemcpyAsync(trace, j->err, sizeof(float) * ne, cudaMemcpyDeviceToHost, j->stream));
+    CU(cudaStreamSynchronize(j->stream));
+    return DWCU_SUCCESS;
+}
+
+int dwcu_job_restore(dwcu_job *j, const float *x, const float *x_prev, const float *trace, const dwcu_job_state *st)
+{
+    if (!j || !x || !st) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    if (!j->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "restore before setup");
+    const bool shb = (j->s.method == DWCU_METHOD_SHB);
+    if (shb && !x_prev) return fail(DWCU_ERROR_INVALID_VALUE, "an SHB snapshot needs x_prev");
+    if (st->volume_elems != j->g.real_elems())
+        return fail(DWCU_ERROR_INVALID_VALUE, "the snapshot is of a job of another size");
+    if (st->bg != j->s.bg) return fail(DWCU_ERROR_INVALID_VALUE, "the snapshot's background differs from the job's");
+    if (st->done_iters < 0 || st->done_iters > trace_cap(j->s) || st->next_iter < -1 ||
+        st->next_iter >= j->it.niter || (st->next_iter >= 0 && st->next_iter != st->done_iters))
+        return fail(DWCU_ERROR_INVALID_VALUE, "inconsistent iteration state (next %d, done %d)", st->next_iter,
+                    st->done_iters);
+    if (st->done_iters > 0 && !trace) return fail(DWCU_ERROR_INVALID_VALUE, "the error trace is missing");
+    CU(cudaSetDevice(j->s.device));
+    const size_t R = sizeof(float) * (size_t) st->volume_elems;
+    CU(cudaMemcpyAsync(j->xa, x, R, cudaMemcpyHostToDevice, j->stream));
+    if (shb) CU(cudaMemcpyAsync(j->xb, x_prev, R, cudaMemcpyHostToDevice, j->stream));
+    if (st->done_iters > 0)
+        CU(cudaMemcpyAsync(j->err, trace, sizeof(float) * st->done_iters, cudaMemcpyHostToDevice, j->stream));
+    CU(cudaStreamSynchronize(j->stream));
+    for (int i = 0; i < st->done_iters; ++i) j->trace[(size_t) i] = trace[i];
+    j->done_iters = st->done_iters;
+    j->k_next = st->next_iter;
+    j->finished = st->next_iter < 0;
+    j->it.iter = st->iter;
+    j->it.error = st->error;
+    j->it.lasterror = st->lasterror;
+    j->spectrum_ready = false;
+    return DWCU_SUCCESS;
+}
+
 const char *dwcu_last_error(void) { return g_last_error.c_str(); }
 int dwcu_abi_version(void) { return DWCU_ABI_VERSION; }
 

@@ -182,6 +182,39 @@ int dwcu_job_set_stream(dwcu_job *job, void *stream);
 /* Device bytes held by the job. */
 int64_t dwcu_job_bytes(const dwcu_job *job);
 
+/* ---------------------------------------------------------------- checkpoints */
+
+/* The state of a job between iterations, for preemption and restarts (the
+ * reference has no checkpoint; its --iterdump images cannot be resumed,
+ * src/method_shb.c:302-322).  The estimates are two padded real volumes of
+ * volume_elems floats: x_k and, for SHB, x_{k-1}. */
+typedef struct dwcu_job_state {
+    int64_t volume_elems;  /* floats per volume */
+    int32_t next_iter;     /* the iteration that runs next; -1 when finished */
+    int32_t done_iters;    /* error values in the trace */
+    int32_t iter;          /* the stopping rule's counter (dw_iterator_t.iter) */
+    float error;           /* the stopping rule's last two error values */
+    float lasterror;
+    float bg;              /* the background the job uses */
+} dwcu_job_state;
+
+/* Copy a set-up job's state to host memory: x_k into x and, for SHB,
+ * x_{k-1} into x_prev (st->volume_elems floats each; with x == NULL only *st
+ * is filled, to learn the size), and the first done_iters error values into
+ * trace (up to trace_capacity; trace may be NULL).  Waits for the job's
+ * queued work. */
+int dwcu_job_snapshot(dwcu_job *job, float *x, float *x_prev, float *trace, int32_t trace_capacity,
+                      dwcu_job_state *st);
+
+/* Continue from a snapshot: `job` was created and set up with the same image,
+ * PSF and options as the job snapshotted (the set-up recomputes the OTF,
+ * weights and background); its estimates, error trace and iteration state
+ * are replaced by the snapshot's, and the next dwcu_job_step continues at
+ * st->next_iter.  DWCU_ERROR_INVALID_VALUE for a snapshot of another job
+ * size or background. */
+int dwcu_job_restore(dwcu_job *job, const float *x, const float *x_prev, const float *trace,
+                     const dwcu_job_state *st);
+
 /* ---------------------------------------------------------------- PSF and tiles */
 
 /* Prepare a PSF for an M x N x P job the way dw_run does before the method
