@@ -12,6 +12,7 @@
 //   y-fwd, z-conv(conj K), y-inv, x[C2R -> update -> next extrapolation -> R2C]
 // i.e. 8 passes over the spectrum and one read/write of the estimates.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>  // header-only: ranges cost a pointer test unless a tool is attached
 
 #include <algorithm>
 #include <atomic>
@@ -108,13 +109,16 @@ static cudaEvent_t prof_event()
     return e;
 }
 
-// bracket one launch: call with begin=true before and begin=false after
+// bracket one launch (the scope's lifetime): CUDA-event timing of the
+// launch's kernel class when profiling is on, and an NVTX range with the
+// class name for trace tools (nsys, ncu --nvtx)
 struct ProfScope {
     bool on = false;
     ProfRec rec{};
     cudaStream_t st = nullptr;
     ProfScope(const char *name, double bytes, cudaStream_t s)
     {
+        nvtxRangePushA(name);
         std::lock_guard<std::mutex> lk(g_prof_mu);
         if (!g_prof_on || g_tuning) return;
         on = true;
@@ -134,11 +138,18 @@ struct ProfScope {
     }
     ~ProfScope()
     {
+        nvtxRangePop();
         if (!on) return;
         cudaEventRecordWithFlags(rec.b, st, capturing(st) ? cudaEventRecordExternal : 0);
         std::lock_guard<std::mutex> lk(g_prof_mu);
         g_prof_recs.push_back(rec);
     }
+};
+
+// an NVTX range over one phase of a job (set-up, iterations, result)
+struct PhaseRange {
+    explicit PhaseRange(const char *name) { nvtxRangePushA(name); }
+    ~PhaseRange() { nvtxRangePop(); }
 };
 
 // ------------------------------------------------------------ plans
@@ -1186,6 +1197,7 @@ static int job_create(long long M, long long N, long long P, long long pM, long 
 // statistics, OTF, weights and the start estimate (method_shb.c:108-296)
 static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_device)
 {
+    PhaseRange pr("dwcu job setup");
     const Geometry &g = j->g;
     CU(cudaSetDevice(j->s.device));
     cudaStream_t st = j->stream;
@@ -1315,6 +1327,7 @@ static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_dev
 static int job_step_impl(dwcu_job *j, int nmax, int *remaining);
 static int job_step(dwcu_job *j, int nmax, int *remaining)
 {
+    PhaseRange pr("dwcu job iterations");
     auto t0 = std::chrono::steady_clock::now();
     int rc = job_step_impl(j, nmax, remaining);
     j->enqueue_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1478,6 +1491,7 @@ static int job_step_impl(dwcu_job *j, int nmax, int *remaining)
 // read; RL's is x_N.  Both live in xa when the loop has finished.
 static int job_result(dwcu_job *j, float *out, bool on_device, dwcu_opts *so)
 {
+    PhaseRange pr("dwcu job result");
     const Geometry &g = j->g;
     CU(cudaSetDevice(j->s.device));
     if (!j->finished) return fail(DWCU_ERROR_NOT_READY, "the job has iterations left");

@@ -428,6 +428,7 @@ static int slab_lowpass_start(dwcu_slab *sl, const float *im)
 // estimate (job_setup's steps, method_shb.c:108-296, over the parts)
 static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
 {
+    PhaseRange pr("dwcu split setup");
     const Geometry &g = sl->g;
     const int n = (int) sl->parts.size();
     const long long npsf = g.pM * g.pN * g.pP;
@@ -631,6 +632,7 @@ static int slab_backward(dwcu_slab *sl, int k, bool next)
 // every iteration (job_step_impl's schedule; launches stay eager)
 static int slab_run(dwcu_slab *sl)
 {
+    PhaseRange pr("dwcu split iterations");
     if (!sl->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "run before setup");
     const bool shb = (sl->s.method == DWCU_METHOD_SHB);
     const bool fixed = (sl->s.iter_type == DWCU_ITER_FIXED);
@@ -677,6 +679,7 @@ static int slab_run(dwcu_slab *sl)
 // the result's image planes from every part into `out` (M x N x P, host)
 static int slab_result(dwcu_slab *sl, float *out, dwcu_opts *so)
 {
+    PhaseRange pr("dwcu split result");
     const Geometry &g = sl->g;
     if (!sl->finished) return fail(DWCU_ERROR_NOT_READY, "the job has iterations left");
     const int n = (int) sl->parts.size();
