@@ -320,6 +320,73 @@ def test_fft_r2c_matches_oracle(shape):
     assert np.max(np.abs(y - x)) < 1e-5
 
 
+def test_fft_round_trip_on_the_reference_kat_sizes():
+    """fft.c:708-780 (`fft_ut`, the reference's FFT unit test): r2c then c2r
+    on sizes 51-60 x 25-34 x 20-29 with values in [5, 6], maximum relative
+    error < 1e-5.  Here every such size with an even x length (the R2C
+    transform's requirement): each one with supported lengths (radices up to
+    16 over 2, 3, 5, 7) round trips within the bound and matches a float64
+    rfftn; the others are refused with DWCU_ERROR_UNSUPPORTED."""
+    import torch
+    rng = np.random.default_rng(11)
+    done = refused = 0
+    for M in range(52, 61, 2):
+        for N in range(25, 35):
+            for P in range(20, 30):
+                x = (5 + rng.random((P, N, M))).astype(np.float32)
+                d_x = _dev(x)
+                d_X = torch.empty((P, N, M // 2 + 1), dtype=torch.complex64, device="cuda")
+                d_y = torch.empty_like(d_x)
+                torch.cuda.synchronize()
+                try:
+                    dw.fft_r2c_device(d_x.data_ptr(), (P, N, M), d_X.data_ptr())
+                except dw.DwcuError as e:
+                    assert e.code == 2, (M, N, P)  # DWCU_ERROR_UNSUPPORTED
+                    refused += 1
+                    continue
+                X = d_X.cpu().numpy()
+                dw.fft_c2r_device(d_X.data_ptr(), (P, N, M), d_y.data_ptr())
+                y = d_y.cpu().numpy() / np.float32(P * N * M)
+                assert np.max(np.abs(y - x) / x) < 1e-5, (M, N, P)
+                ref = np.fft.rfftn(x.astype(np.float64))
+                assert np.max(np.abs(X - ref)) / np.max(np.abs(ref)) < 2e-6, (M, N, P)
+                done += 1
+    assert done == 90 and refused == 410
+
+
+def test_conjugate_product_is_the_circular_correlation():
+    """fft.c:576-628 (`fft_ut_flipall_conj`): ifft(conj(fft(X)) fft(A)) is the
+    circular correlation of A with X -- the convention of the
+    back-projection with the conjugated OTF -- within an MSE of 1e-5 of a
+    float64 computation (relative to the values' scale)."""
+    import torch
+    shape = (15, 14, 12)
+    P, N, M = shape
+    rng = np.random.default_rng(12)
+    X = rng.random(shape).astype(np.float32)
+    A = rng.random(shape).astype(np.float32)
+    spec = []
+    for v in (X, A):
+        d_v = _dev(v)
+        d_S = torch.empty((P, N, M // 2 + 1), dtype=torch.complex64, device="cuda")
+        torch.cuda.synchronize()
+        dw.fft_r2c_device(d_v.data_ptr(), shape, d_S.data_ptr())
+        spec.append(d_S)
+    d_prod = (torch.conj(spec[0]) * spec[1]).contiguous()
+    d_out = torch.empty(shape, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    dw.fft_c2r_device(d_prod.data_ptr(), shape, d_out.data_ptr())
+    out = d_out.cpu().numpy() / np.float32(P * N * M)
+    ref = np.fft.irfftn(np.conj(np.fft.rfftn(X.astype(np.float64))) * np.fft.rfftn(A.astype(np.float64)), s=shape,
+                        axes=(0, 1, 2))
+    # the same thing written as a correlation: sum_n X[n] A[n + k] (circular)
+    k = (3, 5, 7)
+    corr = float(np.sum(X.astype(np.float64) * np.roll(A.astype(np.float64), shift=[-s for s in k], axis=(0, 1, 2))))
+    assert abs(ref[k] - corr) < 1e-9 * abs(corr)
+    assert np.mean((out - ref) ** 2) / np.mean(ref ** 2) < 1e-5
+    assert np.max(np.abs(out - ref)) / np.max(np.abs(ref)) < 1e-5
+
+
 def test_block_reuse_and_release():
     """Jobs of neighbouring sizes reuse cached device blocks; results do not
     depend on which block a job got, and freeing the cache changes nothing."""
