@@ -292,8 +292,6 @@ static long long x_blocks(const Geometry &g) { return g.Z * ((g.Y + g.xp->R - 1)
 struct DeviceCtx {
     int device = -1;
     cudaStream_t stream = nullptr;
-    float *h_err = nullptr;  // pinned slot for per-iteration error readback (one per device)
-    std::mutex h_err_mu;
     std::map<long long, float2 *> tw;  // length -> exp(-2 pi i m / length)
 };
 
@@ -318,7 +316,6 @@ static int get_ctx(int device, DeviceCtx **out)
     auto *c = new DeviceCtx();
     c->device = device;
     CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    CU(cudaMallocHost(&c->h_err, 64 * sizeof(float)));
     g_ctx[device] = c;
     *out = c;
     return DWCU_SUCCESS;
@@ -573,6 +570,11 @@ struct dwcu_job {
     // a part of an image split over GPUs by z planes: the OTF of the part's
     // z-pass columns (all Z planes) takes the place of the spectrum-sized
     // OTF, and T holds the columns being transformed
+    // stopping rules that read the error (REL / ABS): the error values come
+    // back into page-locked slots, one per iteration, each marked by an event
+    float *h_err = nullptr;
+    cudaEvent_t ev_rb[2] = {nullptr, nullptr};
+    int spec = -1;                 // iteration whose forward half is queued ahead of its decision
     long long slab_elems = 0;      // complex elements of each column buffer (0: a whole job)
     bool slab_copies = false;      // the z pass works on gathered copies (T allocated)
     float2 *T = nullptr;
@@ -1184,6 +1186,11 @@ static int job_create(long long M, long long N, long long P, long long pM, long 
         (cudaEventCreate(&j->ev0) != cudaSuccess || cudaEventCreate(&j->ev1) != cudaSuccess ||
          cudaEventCreate(&j->ev2) != cudaSuccess))
         rc = fail(DWCU_ERROR_CUDA, "event creation failed");
+    if (rc == DWCU_SUCCESS && s->iter_type != DWCU_ITER_FIXED &&
+        (cudaMallocHost(&j->h_err, sizeof(float) * (size_t) trace_cap(*s)) != cudaSuccess ||
+         cudaEventCreateWithFlags(&j->ev_rb[0], cudaEventDisableTiming) != cudaSuccess ||
+         cudaEventCreateWithFlags(&j->ev_rb[1], cudaEventDisableTiming) != cudaSuccess))
+        rc = fail(DWCU_ERROR_CUDA, "error read-back slots could not be set up");
     if (rc != DWCU_SUCCESS) {
         dwcu_job_destroy(j);
         return rc;
@@ -1452,16 +1459,33 @@ static int job_step_impl(dwcu_job *j, int nmax, int *remaining)
             if (j->k_next < 0) j->finished = true;
             continue;
         }
-        // REL / ABS: forward half, read the error, decide
-        if (!j->spectrum_ready) TRY(iter_input(j, k));
-        TRY(iter_forward(j, k, true));
-        float e;
-        {
-            std::lock_guard<std::mutex> lk(j->ctx->h_err_mu);
-            CU(cudaMemcpyAsync(j->ctx->h_err, j->err + k, sizeof(float), cudaMemcpyDeviceToHost, j->stream));
-            CU(cudaStreamSynchronize(j->stream));
-            e = *j->ctx->h_err;
+        // REL / ABS (dw.c:237-270): error k decides whether iteration k+1
+        // runs.  Iteration k+1 (the back-projection of k and the forward
+        // half of k+1) is queued before the host waits for error k, so the
+        // GPU does not idle while the host reads and decides.  When the rule
+        // stops at k, the queued work is dropped: SHB's result x_k goes back
+        // to xa by swapping the estimates back, and RL's result x_{k+1} is
+        // the back-projection already computed.
+        auto queue_read = [&](int kk) -> int {
+            CU(cudaMemcpyAsync(j->h_err + kk, j->err + kk, sizeof(float), cudaMemcpyDeviceToHost, j->stream));
+            CU(cudaEventRecord(j->ev_rb[kk & 1], j->stream));
+            return DWCU_SUCCESS;
+        };
+        if (j->spec != k) {
+            if (!j->spectrum_ready) TRY(iter_input(j, k));
+            TRY(iter_forward(j, k, true));
+            TRY(queue_read(k));
         }
+        const bool ahead = (k + 1 < j->it.niter);
+        j->spec = -1;
+        if (ahead) {
+            TRY(iter_backward(j, k, true));
+            TRY(iter_forward(j, k + 1, true));
+            TRY(queue_read(k + 1));
+            j->spec = k + 1;
+        }
+        CU(cudaEventSynchronize(j->ev_rb[k & 1]));
+        const float e = j->h_err[k];
         j->it.set(e);
         j->trace[(size_t) k] = e;
         j->done_iters = k + 1;
@@ -1470,11 +1494,16 @@ static int job_step_impl(dwcu_job *j, int nmax, int *remaining)
         const int kn = j->it.next();
         ran++;
         if (kn >= 0) {
-            TRY(iter_backward(j, k, true));
-            j->spectrum_ready = true;
+            // kn == k + 1 (dw_iterator_next counts up), queued above
+            j->spectrum_ready = false;
             j->k_next = kn;
         } else {
-            if (!shb) TRY(iter_backward(j, k, false));  // RL returns x_{k+1}
+            if (ahead) {
+                if (shb) std::swap(j->xa, j->xb);  // x_k back in xa
+            } else if (!shb) {
+                TRY(iter_backward(j, k, false));  // RL returns x_{k+1}
+            }
+            j->spec = -1;
             j->spectrum_ready = false;
             j->k_next = -1;
             j->finished = true;
@@ -1953,6 +1982,9 @@ void dwcu_job_destroy(dwcu_job *j)
     if (j->ev0) cudaEventDestroy(j->ev0);
     if (j->ev1) cudaEventDestroy(j->ev1);
     if (j->ev2) cudaEventDestroy(j->ev2);
+    for (auto e : j->ev_rb)
+        if (e) cudaEventDestroy(e);
+    if (j->h_err) cudaFreeHost(j->h_err);
     delete j;
 }
 
@@ -2024,6 +2056,7 @@ int dwcu_job_restore(dwcu_job *j, const float *x, const float *x_prev, const flo
     j->it.error = st->error;
     j->it.lasterror = st->lasterror;
     j->spectrum_ready = false;
+    j->spec = -1;
     return DWCU_SUCCESS;
 }
 
