@@ -137,8 +137,18 @@ EXPORTS = [
     "dwcu_tune_plan_info", "dwcu_tune_force", "dwcu_tune_run", "dwcu_tune_query", "dwcu_tune_clear",
     "dwcu_tune_export", "dwcu_tune_import", "dwcu_psf_prepare_device", "dwcu_selftest_bounded_wait",
     "dwcu_debug_guards", "dwcu_debug_guard_violations", "dwcu_deconvolve_slabs", "dwcu_slab_layout",
-    "dwcu_job_snapshot", "dwcu_job_restore",
+    "dwcu_job_snapshot", "dwcu_job_restore", "dwcu_slab_part_create", "dwcu_slab_part_export",
+    "dwcu_slab_part_import", "dwcu_slab_part_run", "dwcu_slab_destroy",
 ]
+
+# the collectives a process-per-part split calls back (dwcu_slab_sync)
+SLAB_BARRIER = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p)
+SLAB_ALLREDUCE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32)
+
+
+class SlabSync(ctypes.Structure):
+    """dwcu_slab_sync."""
+    _fields_ = [("barrier", SLAB_BARRIER), ("allreduce", SLAB_ALLREDUCE), ("ctx", ctypes.c_void_p)]
 
 # pass kinds of the autotuner (dwcu.h)
 PLAN_LINES, PLAN_Y, PLAN_X = 0, 1, 2
@@ -170,6 +180,17 @@ def lib() -> ctypes.CDLL:
     L.dwcu_deconvolve_slabs.restype = ctypes.c_int
     L.dwcu_slab_layout.argtypes = [i64, i64, i64, i64, i64, i64, i32, i32, i32, ctypes.POINTER(i64)]
     L.dwcu_slab_layout.restype = ctypes.c_int
+    L.dwcu_slab_part_create.argtypes = [i64, i64, i64, i64, i64, i64, P_opts, i32, i32, vp, ctypes.POINTER(SlabSync),
+                                        ctypes.POINTER(vp)]
+    L.dwcu_slab_part_create.restype = ctypes.c_int
+    L.dwcu_slab_part_export.argtypes = [vp, vp, ctypes.POINTER(i64)]
+    L.dwcu_slab_part_export.restype = ctypes.c_int
+    L.dwcu_slab_part_import.argtypes = [vp, i32, vp, i64]
+    L.dwcu_slab_part_import.restype = ctypes.c_int
+    L.dwcu_slab_part_run.argtypes = [vp, vp, vp, vp, P_opts]
+    L.dwcu_slab_part_run.restype = ctypes.c_int
+    L.dwcu_slab_destroy.argtypes = [vp]
+    L.dwcu_slab_destroy.restype = None
     L.dwcu_release_cache.argtypes = [i32]
     L.dwcu_release_cache.restype = ctypes.c_int
     L.dwcu_job_create.argtypes = [i64, i64, i64, i64, i64, i64, P_opts, ctypes.POINTER(vp)]
@@ -350,6 +371,74 @@ def run_slabs(im: np.ndarray, psf: np.ndarray, parts: int = 2, devices=None, out
     _check(lib().dwcu_deconvolve_slabs(im.ctypes.data, M, N, P, psf.ctypes.data, pM, pN, pP, ctypes.byref(o),
                                        parts, dev, out.ctypes.data))
     return Result(out, trace[: o.iterations_done].copy(), o)
+
+
+class SlabPart:
+    """This process's part of an image split over processes (dwcu_slab_part_*).
+    ``barrier(stream)`` and ``allreduce(stream, n, op)`` are the caller's
+    collectives (see dwcu.h); ``sync_buf`` a device buffer of at least 4
+    doubles that ``allreduce`` reduces in place."""
+
+    def __init__(self, shape, psf_shape, parts: int, part: int, sync_buf: int, barrier, allreduce, **kw):
+        self.shape = tuple(shape)
+        self.opts = make_opts(**kw)
+
+        def _barrier(ctx, stream):
+            try:
+                barrier(stream or 0)
+                return 0
+            except Exception:
+                return 1
+
+        def _allreduce(ctx, stream, n, op):
+            try:
+                allreduce(stream or 0, int(n), int(op))
+                return 0
+            except Exception:
+                return 1
+
+        self._cb = (SLAB_BARRIER(_barrier), SLAB_ALLREDUCE(_allreduce))  # kept alive while the part lives
+        self._sync = SlabSync(self._cb[0], self._cb[1], None)
+        P, N, M = self.shape
+        pP, pN, pM = psf_shape
+        h = ctypes.c_void_p()
+        _check(lib().dwcu_slab_part_create(M, N, P, pM, pN, pP, ctypes.byref(self.opts), parts, part,
+                                           ctypes.c_void_p(sync_buf), ctypes.byref(self._sync), ctypes.byref(h)))
+        self.h = h
+
+    def export(self):
+        """(IPC handle bytes, spectrum offset) for the other processes."""
+        buf = ctypes.create_string_buffer(64)
+        off = ctypes.c_int64()
+        _check(lib().dwcu_slab_part_export(self.h, buf, ctypes.byref(off)))
+        return buf.raw, off.value
+
+    def import_part(self, part: int, handle: bytes, offset: int) -> None:
+        buf = ctypes.create_string_buffer(bytes(handle), 64)
+        _check(lib().dwcu_slab_part_import(self.h, part, buf, offset))
+
+    def run(self, im: np.ndarray, psf: np.ndarray, out: np.ndarray) -> Result:
+        """Set-up, iterations and this part's image planes into ``out``."""
+        im = np.ascontiguousarray(im, dtype=np.float32)
+        psf = np.ascontiguousarray(psf, dtype=np.float32)
+        o = self.opts
+        cap = max(o.n_iter, o.maxiter, 1)
+        trace = np.zeros(cap, dtype=np.float32)
+        o.error_trace = trace.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        o.trace_capacity = cap
+        _check(lib().dwcu_slab_part_run(self.h, im.ctypes.data, psf.ctypes.data, out.ctypes.data, ctypes.byref(o)))
+        return Result(out, trace[: o.iterations_done].copy(), o)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().dwcu_slab_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def slab_layout(shape, psf_shape, parts: int, part: int, border_quality: int = 2) -> dict:

@@ -1124,17 +1124,23 @@ static int tuned_choice(DeviceCtx *ctx, int kind, int n, int *rc_out = nullptr)
 }
 
 // the geometry's plans: candidate 0 from make_geometry, replaced by the
-// tuned choice of each pass's length
-static void tune_geometry(DeviceCtx *ctx, Geometry &g)
+// tuned choice of each pass's length (measure: false -- recorded choices
+// only, e.g. an imported plan table, never a new measurement)
+static void tune_geometry(DeviceCtx *ctx, Geometry &g, bool measure = true)
 {
+    auto choice = [&](int kind, int n) {
+        if (measure) return tuned_choice(ctx, kind, n);
+        const int c = tune_lookup(ctx->device, kind, n);
+        return c >= 0 && c < tune_plan_count(kind, n) ? c : 0;
+    };
     const int nx = (int) (g.X / 2);
-    if (const XPlan *p = x_plan(nx, tuned_choice(ctx, DWCU_PLAN_X, nx))) g.xp = p;
+    if (const XPlan *p = x_plan(nx, choice(DWCU_PLAN_X, nx))) g.xp = p;
     if (g.ytp) {
-        if (const YPlan *p = y_plan((int) g.Y, tuned_choice(ctx, DWCU_PLAN_Y, (int) g.Y))) g.ytp = p;
+        if (const YPlan *p = y_plan((int) g.Y, choice(DWCU_PLAN_Y, (int) g.Y))) g.ytp = p;
     } else if (g.yp) {
-        if (const LinesPlan *p = lines_plan((int) g.Y, tuned_choice(ctx, DWCU_PLAN_LINES, (int) g.Y))) g.yp = p;
+        if (const LinesPlan *p = lines_plan((int) g.Y, choice(DWCU_PLAN_LINES, (int) g.Y))) g.yp = p;
     }
-    if (const LinesPlan *p = lines_plan((int) g.Z, tuned_choice(ctx, DWCU_PLAN_LINES, (int) g.Z))) g.zp = p;
+    if (const LinesPlan *p = lines_plan((int) g.Z, choice(DWCU_PLAN_LINES, (int) g.Z))) g.zp = p;
 }
 
 static long long job_bytes_estimate(const Geometry &g, const dwcu_opts &s)

@@ -25,11 +25,13 @@
 // where the GPUs have no peer access).  The OTF of the part's columns stays
 // with the part ([Z][nc]).
 //
-// Order between parts (slab_barrier): before a gather, every part's writes of
-// the planes it gathers are complete; before the y pass after a scatter,
-// every part's scatter is complete.  Each part records an event and waits on
-// every other part's.  Within one transpose, part p reads and then writes
-// the same region (its columns of every plane), which no other part touches.
+// Order between parts (slab_barrier): before the z pass, every part's y pass
+// is complete; before the y pass after it, every part's z pass (or scatter)
+// is complete.  Parts driven by one process: each part records an event and
+// waits on every other part's.  One process per part (dwcu_slab_part_*): the
+// caller's barrier, a stream-ordered collective such as an NCCL all-reduce,
+// and the peers' spectra mapped through CUDA IPC handles.  During a z pass,
+// part p reads and writes only its own columns, which no other part touches.
 //
 // Supported: SHB and RL, every stopping rule, every start (the low-pass
 // start smooths the whole image on part 0's GPU and deals its planes out),
@@ -51,6 +53,8 @@ struct SlabPart {
     cudaEvent_t ev = nullptr;      // ordering between parts
     double *psum = nullptr;        // per iteration: the error sum of the part's tiles
     float2 **planes = nullptr;     // planes mode: the address of every plane z (on this part's GPU)
+    float2 *S = nullptr;           // the part's spectrum planes (its own, or mapped from another process)
+    void *ipc_base = nullptr;      // the mapped allocation of another process's part
 };
 
 // the planes and z-pass columns of part p of n (host arithmetic only)
@@ -120,6 +124,12 @@ struct dwcu_slab {
     std::vector<dwcu::SlabPart> parts;
     double *sums = nullptr;        // on part 0's device: the parts' error sums of one iteration
     bool copies = false;           // z pass on gathered copies instead of in place
+    int local = -1;                // one process per part: the part this process holds (-1: all)
+    dwcu_slab_sync sync{};         // ... and the caller's collectives
+    double *sync_buf = nullptr;    // ... on a device buffer of the caller's
+    // the part that times the run and holds the error trace: part 0, or the
+    // process's own part
+    dwcu::SlabPart &lead() { return parts[(size_t) (local >= 0 ? local : 0)]; }
     dwcu::Iter it;
     int k_next = -1;
     bool spectrum_ready = false;
@@ -137,6 +147,11 @@ static void slab_destroy(dwcu_slab *sl)
         if (pt.stream) {
             cudaSetDevice(pt.device);
             cudaStreamSynchronize(pt.stream);
+        }
+    for (auto &pt : sl->parts)
+        if (pt.ipc_base) {
+            cudaSetDevice(sl->lead().device);
+            cudaIpcCloseMemHandle(pt.ipc_base);
         }
     for (auto &pt : sl->parts) {
         if (pt.device < 0) continue;
@@ -180,6 +195,7 @@ static int slab_part_create(dwcu_slab *sl, int p, int device)
     j->slab_elems = g.Z * pt.nc;
     j->slab_copies = sl->copies;
     TRY(alloc_job(j));
+    pt.S = j->S;
     TRY(get_twiddles(ctx, g.X, &j->tw_x));
     TRY(get_twiddles(ctx, g.X / 2, &j->tw_l));
     if (g.Y > 1) TRY(get_twiddles(ctx, g.Y, &j->tw_y));
@@ -238,19 +254,6 @@ static int slab_create(long long M, long long N, long long P, long long pM, long
             if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) rc = fail(DWCU_ERROR_CUDA, "peer access %d -> %d: %s", a, b, cudaGetErrorString(e));
             cudaGetLastError();
         }
-    // planes mode: every part's table of the Z planes' addresses
-    if (rc == DWCU_SUCCESS && !sl->copies) {
-        const long long plane = g.NKB * g.Y * KB;
-        std::vector<float2 *> tab((size_t) g.Z);
-        for (long long z = 0; z < g.Z; ++z) tab[(size_t) z] = sl->parts[(size_t) (z % nparts)].j->S + (z / nparts) * plane;
-        for (auto &pt : sl->parts) {
-            if (rc != DWCU_SUCCESS) break;
-            cudaSetDevice(pt.device);
-            if (cudaMalloc(&pt.planes, sizeof(float2 *) * (size_t) g.Z) != cudaSuccess ||
-                cudaMemcpy(pt.planes, tab.data(), sizeof(float2 *) * (size_t) g.Z, cudaMemcpyHostToDevice) != cudaSuccess)
-                rc = fail(DWCU_ERROR_OUT_OF_MEMORY, "the plane table could not be set up");
-        }
-    }
     if (rc == DWCU_SUCCESS) {
         cudaSetDevice(dev0);
         if (cudaMalloc(&sl->sums, sizeof(double) * (size_t) nparts) != cudaSuccess)
@@ -264,9 +267,51 @@ static int slab_create(long long M, long long N, long long P, long long pM, long
     return DWCU_SUCCESS;
 }
 
+// planes mode: each own part's table of the Z planes' addresses (once every
+// part's spectrum is known)
+static int slab_plane_tables(dwcu_slab *sl)
+{
+    if (sl->copies) return DWCU_SUCCESS;
+    const Geometry &g = sl->g;
+    const long long n = (long long) sl->parts.size();
+    const long long plane = g.NKB * g.Y * KB;
+    std::vector<float2 *> tab((size_t) g.Z);
+    for (long long z = 0; z < g.Z; ++z) {
+        float2 *S = sl->parts[(size_t) (z % n)].S;
+        if (!S) return fail(DWCU_ERROR_INVALID_VALUE, "part %lld's spectrum is not mapped (dwcu_slab_part_import)", z % n);
+        tab[(size_t) z] = S + (z / n) * plane;
+    }
+    for (auto &pt : sl->parts) {
+        if (!pt.j || pt.planes) continue;
+        CU(cudaSetDevice(pt.device));
+        CU(cudaMalloc(&pt.planes, sizeof(float2 *) * (size_t) g.Z));
+        CU(cudaMemcpy(pt.planes, tab.data(), sizeof(float2 *) * (size_t) g.Z, cudaMemcpyHostToDevice));
+    }
+    return DWCU_SUCCESS;
+}
+
+// the caller's collectives (one process per part)
+static int slab_sync_barrier(dwcu_slab *sl)
+{
+    SlabPart &me = sl->lead();
+    CU(cudaSetDevice(me.device));
+    if (sl->sync.barrier(sl->sync.ctx, (void *) me.stream) != 0)
+        return fail(DWCU_ERROR_INTERNAL, "the caller's barrier failed");
+    return DWCU_SUCCESS;
+}
+static int slab_sync_allreduce(dwcu_slab *sl, int n, int op)
+{
+    SlabPart &me = sl->lead();
+    CU(cudaSetDevice(me.device));
+    if (sl->sync.allreduce(sl->sync.ctx, (void *) me.stream, n, op) != 0)
+        return fail(DWCU_ERROR_INTERNAL, "the caller's all-reduce failed");
+    return DWCU_SUCCESS;
+}
+
 // every part waits until every other part has reached this point
 static int slab_barrier(dwcu_slab *sl)
 {
+    if (sl->local >= 0) return slab_sync_barrier(sl);
     if (sl->parts.size() < 2) return DWCU_SUCCESS;
     for (auto &pt : sl->parts) {
         CU(cudaSetDevice(pt.device));
@@ -280,9 +325,11 @@ static int slab_barrier(dwcu_slab *sl)
     return DWCU_SUCCESS;
 }
 
-// part 0 waits until every part has reached this point
+// part 0 waits until every part has reached this point (one process per
+// part: every part waits)
 static int slab_join0(dwcu_slab *sl)
 {
+    if (sl->local >= 0) return slab_sync_barrier(sl);
     if (sl->parts.size() < 2) return DWCU_SUCCESS;
     for (size_t p = 1; p < sl->parts.size(); ++p) {
         CU(cudaSetDevice(sl->parts[p].device));
@@ -306,7 +353,7 @@ static int slab_transpose(dwcu_slab *sl, SlabPart &pt, float2 *buf, bool image_o
         const long long h = image_only ? o.pl : o.zl;
         if (h == 0) continue;
         float2 *cols = buf + q * pt.nc;    // rows q, q+n, ... of [Z][nc]
-        float2 *planes = o.j->S + pt.c0;   // the part's planes, this part's columns
+        float2 *planes = o.S + pt.c0;      // the part's planes, this part's columns
         const size_t cp = sizeof(float2) * (size_t) (n * pt.nc), pp = sizeof(float2) * (size_t) plane;
         const size_t w = sizeof(float2) * (size_t) pt.nc;
         if (scatter)
@@ -332,6 +379,7 @@ static int slab_conv(dwcu_slab *sl, int conj, bool in_img, bool out_img)
 {
     const Geometry &g = sl->g;
     for (auto &pt : sl->parts) {
+        if (!pt.j) continue;
         CU(cudaSetDevice(pt.device));
         const long long h = in_img ? pt.pl : pt.zl;
         if (h > 0) TRY(pass_y(pt.j, LINES_FWD, pt.j->S, h));
@@ -339,6 +387,7 @@ static int slab_conv(dwcu_slab *sl, int conj, bool in_img, bool out_img)
     TRY(slab_barrier(sl));
     const int mode = conj ? LINES_CONV_CONJ : LINES_CONV;
     for (auto &pt : sl->parts) {
+        if (!pt.j) continue;
         if (sl->copies) {
             TRY(slab_transpose(sl, pt, pt.j->T, in_img, false));
             TRY(slab_zpass(sl, pt, mode, pt.j->T, in_img ? g.P : g.Z, out_img ? g.P : g.Z));
@@ -351,6 +400,7 @@ static int slab_conv(dwcu_slab *sl, int conj, bool in_img, bool out_img)
     }
     TRY(slab_barrier(sl));
     for (auto &pt : sl->parts) {
+        if (!pt.j) continue;
         CU(cudaSetDevice(pt.device));
         const long long h = out_img ? pt.pl : pt.zl;
         if (h > 0) TRY(pass_y(pt.j, LINES_INV, pt.j->S, h));
@@ -360,15 +410,16 @@ static int slab_conv(dwcu_slab *sl, int conj, bool in_img, bool out_img)
 
 // The low-pass start (method_shb.c:278-285, method_rl.c:290-297): the image
 // smoothed by fim_gsmooth (sigma 8) along x, y and z -- the z smoothing
-// needs whole image columns, so the whole image is smoothed on part 0's GPU
-// (job_setup's kernels and taps) -- then each part's image planes are copied
-// into the corner of its zeroed x_0.
+// needs whole image columns, so the whole image is smoothed on one GPU
+// (part 0's, or with one process per part each process's own; job_setup's
+// kernels and taps) -- then each part's image planes are copied into the
+// corner of its zeroed x_0.
 static int slab_lowpass_start(dwcu_slab *sl, const float *im)
 {
     if (sl->s.start_condition != DWCU_START_LP) return DWCU_SUCCESS;
     const Geometry &g = sl->g;
     const int n = (int) sl->parts.size();
-    SlabPart &p0 = sl->parts[0];
+    SlabPart &p0 = sl->lead();
     CU(cudaSetDevice(p0.device));
     const long long nimg = g.M * g.N * g.P;
     float *t = nullptr;
@@ -402,8 +453,9 @@ static int slab_lowpass_start(dwcu_slab *sl, const float *im)
         for (int p = 0; p < n; ++p) {
             SlabPart &pt = sl->parts[(size_t) p];
             dwcu_job *j = pt.j;
+            if (!j) continue;
             CU(cudaSetDevice(pt.device));
-            if (p > 0) CU(cudaStreamWaitEvent(pt.stream, p0.ev, 0));
+            if (&pt != &p0) CU(cudaStreamWaitEvent(pt.stream, p0.ev, 0));
             CU(cudaMemsetAsync(j->xa, 0, sizeof(float) * (size_t) j->g.real_elems(), pt.stream));
             for (long long l = 0; l < pt.pl; ++l) {
                 const long long z = l * n + p;
@@ -416,6 +468,7 @@ static int slab_lowpass_start(dwcu_slab *sl, const float *im)
     rc = run();
     // the work space is freed once every part's copies are done
     for (auto &pt : sl->parts) {
+        if (!pt.j) continue;
         cudaSetDevice(pt.device);
         cudaStreamSynchronize(pt.stream);
     }
@@ -433,12 +486,14 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
     const int n = (int) sl->parts.size();
     const long long npsf = g.pM * g.pN * g.pP;
     const unsigned long long wmnp = (unsigned long long) (g.wM * g.wN * g.wP);
+    TRY(slab_plane_tables(sl));
     for (int p = 0; p < n; ++p) {
         SlabPart &pt = sl->parts[(size_t) p];
         dwcu_job *j = pt.j;
+        if (!j) continue;
         CU(cudaSetDevice(pt.device));
         cudaStream_t st = pt.stream;
-        if (p == 0) CU(cudaEventRecord(j->ev0, st));
+        if (&pt == &sl->lead()) CU(cudaEventRecord(j->ev0, st));
         for (long long l = 0; l < pt.pl; ++l) {
             const long long z = l * n + p;
             CU(cudaMemcpy2DAsync(j->gimg + l * g.N * g.GP, sizeof(float) * g.GP, im + z * g.M * g.N,
@@ -468,6 +523,7 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
     float gmin = INFINITY;
     int flags = 0;
     for (auto &pt : sl->parts) {
+        if (!pt.j) continue;
         JobScalars hs{};
         CU(cudaSetDevice(pt.device));
         CU(cudaMemcpyAsync(&hs, pt.j->sc, sizeof hs, cudaMemcpyDeviceToHost, pt.stream));
@@ -478,12 +534,31 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
             gmin = std::fmin(gmin, hs.gmin);
         }
     }
+    if (sl->local >= 0) {
+        // over the processes: the image sum and the parts with non-finite
+        // image or PSF values added, the minimum taken
+        SlabPart &me = sl->lead();
+        double v[3] = {sumg, (double) (flags & 1), (double) ((flags >> 1) & 1)};
+        CU(cudaSetDevice(me.device));
+        CU(cudaMemcpyAsync(sl->sync_buf, v, sizeof v, cudaMemcpyHostToDevice, me.stream));
+        TRY(slab_sync_allreduce(sl, 3, 0));
+        CU(cudaMemcpyAsync(v, sl->sync_buf, sizeof v, cudaMemcpyDeviceToHost, me.stream));
+        CU(cudaStreamSynchronize(me.stream));
+        sumg = v[0];
+        flags = (v[1] > 0 ? 1 : 0) | (v[2] > 0 ? 2 : 0);
+        double m = (double) gmin;
+        CU(cudaMemcpyAsync(sl->sync_buf, &m, sizeof m, cudaMemcpyHostToDevice, me.stream));
+        TRY(slab_sync_allreduce(sl, 1, 1));
+        CU(cudaMemcpyAsync(&m, sl->sync_buf, sizeof m, cudaMemcpyDeviceToHost, me.stream));
+        CU(cudaStreamSynchronize(me.stream));
+        gmin = (float) m;
+    }
     if (flags & 1) return fail(DWCU_ERROR_INPUT, "the image contains non-finite values");
     if (flags & 2) return fail(DWCU_ERROR_INPUT, "the PSF contains non-finite values");
     if (g.wx || g.wy) {
         // the periodic margins assume the PSF maximum within h of both ends (as job_setup)
         long long am = 0;
-        SlabPart &p0 = sl->parts[0];
+        SlabPart &p0 = sl->lead();
         CU(cudaSetDevice(p0.device));
         CU(cudaMemcpy(&am, p0.j->amax, sizeof am, cudaMemcpyDeviceToHost));
         const long long ax = am % g.pM, ay = (am / g.pM) % g.pN;
@@ -505,6 +580,7 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
     for (int p = 0; p < n; ++p) {
         SlabPart &pt = sl->parts[(size_t) p];
         dwcu_job *j = pt.j;
+        if (!j) continue;
         CU(cudaSetDevice(pt.device));
         cudaStream_t st = pt.stream;
         CU(cudaMemcpyAsync(j->sc, &all, sizeof all, cudaMemcpyHostToDevice, st));
@@ -522,19 +598,22 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
     // ... and the z transform of the part's columns, kept as its OTF
     TRY(slab_barrier(sl));
     for (auto &pt : sl->parts) {
+        if (!pt.j) continue;
         TRY(slab_transpose(sl, pt, pt.j->K, false, false));
         TRY(slab_zpass(sl, pt, LINES_FWD, pt.j->K, g.Z, g.Z));
     }
     TRY(slab_barrier(sl));  // every gather has read the spectra before they change
 
     // Bertero weights: W = 1/P1 where P1 = K^T 1_image > 0.01 (method_shb.c:216-235)
-    if (sl->parts[0].j->W) {
+    if (sl->lead().j->W) {
         for (auto &pt : sl->parts) {
+            if (!pt.j) continue;
             CU(cudaSetDevice(pt.device));
             TRY(pass_x(pt.j, XOP_FWD_ONES, 1, pt.j->S, nullptr, nullptr, nullptr, 0, 0));
         }
         TRY(slab_conv(sl, 1, false, false));
         for (auto &pt : sl->parts) {
+            if (!pt.j) continue;
             CU(cudaSetDevice(pt.device));
             TRY(pass_x(pt.j, XOP_WEIGHTS, 0, pt.j->S, nullptr, nullptr, pt.j->W, 0, 0));
         }
@@ -543,6 +622,7 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
     TRY(slab_lowpass_start(sl, im));
     for (auto &pt : sl->parts) {
         dwcu_job *j = pt.j;
+        if (!j) continue;
         CU(cudaSetDevice(pt.device));
         cudaStream_t st = pt.stream;
         const long long nv = j->g.real_elems();
@@ -568,8 +648,8 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
     sl->done_iters = 0;
     sl->setup_done = true;
     TRY(slab_join0(sl));
-    CU(cudaSetDevice(sl->parts[0].device));
-    CU(cudaEventRecord(sl->parts[0].j->ev1, sl->parts[0].stream));
+    CU(cudaSetDevice(sl->lead().device));
+    CU(cudaEventRecord(sl->lead().j->ev1, sl->lead().stream));
     return DWCU_SUCCESS;
 }
 
@@ -577,6 +657,7 @@ static int slab_setup(dwcu_slab *sl, const float *im, const float *psf)
 static int slab_input(dwcu_slab *sl, int k)
 {
     for (auto &pt : sl->parts) {
+        if (!pt.j) continue;
         CU(cudaSetDevice(pt.device));
         TRY(iter_input(pt.j, k));
     }
@@ -584,7 +665,8 @@ static int slab_input(dwcu_slab *sl, int k)
 }
 
 // forward half of iteration k (iter_forward over the parts): y = K p_k,
-// error_k on part 0; with `ratio`, the ratio's transform
+// error_k on part 0 (with one process per part: on every part, from the
+// caller's all-reduce of the parts' sums); with `ratio`, the ratio's transform
 static int slab_forward(dwcu_slab *sl, int k, bool ratio)
 {
     const Geometry &g = sl->g;
@@ -593,11 +675,21 @@ static int slab_forward(dwcu_slab *sl, int k, bool ratio)
     const int op = ratio ? (shb ? XOP_RATIO_SHB : XOP_RATIO_RL) : XOP_ERROR_ONLY;
     const long long ytiles = (g.Y + g.xp->R - 1) / g.xp->R;
     for (auto &pt : sl->parts) {
+        if (!pt.j) continue;
         CU(cudaSetDevice(pt.device));
         const long long tiles = (op == XOP_RATIO_RL) ? pt.j->nxb : pt.pl * ytiles;
         if (tiles > 0) TRY(pass_x(pt.j, op, ratio ? 1 : 0, pt.j->S, nullptr, nullptr, nullptr, 0, 0, tiles));
         k_slab_err_sum<<<1, kRedThreads, 0, pt.stream>>>(pt.j->partial, (int) tiles, pt.psum + k);
         CHECK_LAUNCH();
+    }
+    if (sl->local >= 0) {
+        SlabPart &me = sl->lead();
+        CU(cudaSetDevice(me.device));
+        CU(cudaMemcpyAsync(sl->sync_buf, me.psum + k, sizeof(double), cudaMemcpyDeviceToDevice, me.stream));
+        TRY(slab_sync_allreduce(sl, 1, 0));
+        k_slab_err_combine<<<1, 32, 0, me.stream>>>(sl->sync_buf, 1, (double) (g.M * g.N * g.P), me.j->err + k);
+        CHECK_LAUNCH();
+        return DWCU_SUCCESS;
     }
     TRY(slab_join0(sl));
     SlabPart &p0 = sl->parts[0];
@@ -617,6 +709,7 @@ static int slab_backward(dwcu_slab *sl, int k, bool next)
     TRY(slab_conv(sl, 1, shb, false));
     for (auto &pt : sl->parts) {
         dwcu_job *j = pt.j;
+        if (!j) continue;
         CU(cudaSetDevice(pt.device));
         if (shb) {
             TRY(pass_x(j, XOP_UPDATE_SHB, next ? 1 : 0, j->S, j->xa, j->xb, j->xb, shb_alpha(k, sl->s.alphamax),
@@ -636,7 +729,7 @@ static int slab_run(dwcu_slab *sl)
     if (!sl->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "run before setup");
     const bool shb = (sl->s.method == DWCU_METHOD_SHB);
     const bool fixed = (sl->s.iter_type == DWCU_ITER_FIXED);
-    SlabPart &p0 = sl->parts[0];
+    SlabPart &p0 = sl->lead();
     while (!sl->finished) {
         const int k = sl->k_next;
         if (fixed) {
@@ -683,13 +776,14 @@ static int slab_result(dwcu_slab *sl, float *out, dwcu_opts *so)
     const Geometry &g = sl->g;
     if (!sl->finished) return fail(DWCU_ERROR_NOT_READY, "the job has iterations left");
     const int n = (int) sl->parts.size();
-    SlabPart &p0 = sl->parts[0];
+    SlabPart &p0 = sl->lead();
     TRY(slab_join0(sl));
     CU(cudaSetDevice(p0.device));
     CU(cudaEventRecord(p0.j->ev2, p0.stream));
     int flags = 0;
     for (int p = 0; p < n; ++p) {
         SlabPart &pt = sl->parts[(size_t) p];
+        if (!pt.j) continue;
         CU(cudaSetDevice(pt.device));
         for (long long l = 0; l < pt.pl; ++l) {
             const long long z = l * n + p;
@@ -726,9 +820,112 @@ static int slab_result(dwcu_slab *sl, float *out, dwcu_opts *so)
     return DWCU_SUCCESS;
 }
 
+// one part of a job split over processes (one per GPU): this process's
+// part on s->device; the other parts' spectra come from
+// dwcu_slab_part_import
+static int slab_create_part(long long M, long long N, long long P, long long pM, long long pN, long long pP,
+                            const dwcu_opts *s, int nparts, int part, double *sync_buf, const dwcu_slab_sync *sync,
+                            dwcu_slab **out)
+{
+    *out = nullptr;
+    if (!s || !sync || !sync->barrier || !sync->allreduce || !sync_buf)
+        return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    TRY(check_opts(*s));
+    if (nparts < 1 || nparts > 64 || part < 0 || part >= nparts)
+        return fail(DWCU_ERROR_INVALID_VALUE, "part %d of %d", part, nparts);
+    Geometry g;
+    TRY(make_geometry(M, N, P, pM, pN, pP, s->border_quality, g));
+    if (g.wz)
+        return fail(DWCU_ERROR_UNSUPPORTED, "job z size %lld needs periodic margins along z: not with parts", g.wP);
+    if (nparts > g.Z) return fail(DWCU_ERROR_UNSUPPORTED, "%d parts for %lld z planes", nparts, g.Z);
+    if (g.NKB * g.Y < nparts) return fail(DWCU_ERROR_UNSUPPORTED, "too few z-pass columns for %d parts", nparts);
+    DeviceCtx *ctx = nullptr;
+    TRY(get_ctx(s->device, &ctx));
+    CU(cudaSetDevice(s->device));
+    // every process must run the same plans: recorded choices (an imported
+    // plan table) or the heuristic ones, never a measurement of its own
+    tune_geometry(ctx, g, false);
+    dwcu_slab *sl = new dwcu_slab();
+    sl->s = *s;
+    sl->g = g;
+    sl->parts.resize((size_t) nparts);
+    sl->local = part;
+    sl->sync = *sync;
+    sl->sync_buf = sync_buf;
+    const char *tr = getenv("DWCU_SLAB_TRANSPOSE");
+    sl->copies = tr && strcmp(tr, "copy") == 0;
+    for (int p = 0; p < nparts; ++p) {
+        SlabPart &o = sl->parts[(size_t) p];
+        slab_layout(g.Z, g.P, g.NKB * g.Y * KB, nparts, p, &o.zl, &o.pl, &o.c0, &o.nc);
+    }
+    const int rc = slab_part_create(sl, part, s->device);
+    if (rc != DWCU_SUCCESS) {
+        slab_destroy(sl);
+        return rc;
+    }
+    *out = sl;
+    return DWCU_SUCCESS;
+}
+
 }  // namespace dwcu
 
 extern "C" {
+
+int dwcu_slab_part_create(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP, const dwcu_opts *s,
+                          int32_t nparts, int32_t part, double *sync_buf, const dwcu_slab_sync *sync, dwcu_slab **out)
+{
+    if (!out) return fail(DWCU_ERROR_INVALID_VALUE, "out is NULL");
+    return slab_create_part(M, N, P, pM, pN, pP, s, nparts, part, sync_buf, sync, out);
+}
+
+int dwcu_slab_part_export(dwcu_slab *sl, void *handle, int64_t *offset)
+{
+    if (!sl || !handle || !offset || sl->local < 0) return fail(DWCU_ERROR_INVALID_VALUE, "not a part of a split over processes");
+    SlabPart &me = sl->lead();
+    CU(cudaSetDevice(me.device));
+    cudaIpcMemHandle_t h;
+    CU(cudaIpcGetMemHandle(&h, me.j->base));
+    memcpy(handle, &h, sizeof h);
+    *offset = (int64_t) ((char *) me.j->S - me.j->base);
+    return DWCU_SUCCESS;
+}
+
+int dwcu_slab_part_import(dwcu_slab *sl, int32_t part, const void *handle, int64_t offset)
+{
+    if (!sl || !handle || sl->local < 0) return fail(DWCU_ERROR_INVALID_VALUE, "not a part of a split over processes");
+    if (part < 0 || part >= (int) sl->parts.size() || part == sl->local)
+        return fail(DWCU_ERROR_INVALID_VALUE, "part %d: not another part of this split", part);
+    SlabPart &o = sl->parts[(size_t) part];
+    if (o.ipc_base) return fail(DWCU_ERROR_INVALID_VALUE, "part %d is mapped already", part);
+    CU(cudaSetDevice(sl->lead().device));
+    cudaIpcMemHandle_t h;
+    memcpy(&h, handle, sizeof h);
+    void *base = nullptr;
+    CU(cudaIpcOpenMemHandle(&base, h, cudaIpcMemLazyEnablePeerAccess));
+    o.ipc_base = base;
+    o.S = reinterpret_cast<float2 *>((char *) base + offset);
+    return DWCU_SUCCESS;
+}
+
+int dwcu_slab_part_run(dwcu_slab *sl, const float *im, const float *psf, float *out, dwcu_opts *so)
+{
+    if (!sl || !im || !psf || !out) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
+    if (sl->local < 0) return fail(DWCU_ERROR_INVALID_VALUE, "not a part of a split over processes");
+    if (sl->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "the part has run already");
+    if (so) so->iterations_done = 0;
+    int rc = slab_setup(sl, im, psf);
+    if (rc == DWCU_SUCCESS) rc = slab_run(sl);
+    if (rc == DWCU_SUCCESS) rc = slab_result(sl, out, so);
+    // no process frees or reuses its memory while another may still read it
+    if (rc == DWCU_SUCCESS) rc = slab_sync_barrier(sl);
+    if (rc == DWCU_SUCCESS) {
+        CU(cudaSetDevice(sl->lead().device));
+        CU(cudaStreamSynchronize(sl->lead().stream));
+    }
+    return rc;
+}
+
+void dwcu_slab_destroy(dwcu_slab *sl) { slab_destroy(sl); }
 
 int dwcu_slab_layout(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP, int32_t border_quality,
                      int32_t nparts, int32_t part, int64_t *info)

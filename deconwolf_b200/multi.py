@@ -151,3 +151,71 @@ def deconvolve_tiled(im: np.ndarray, psf: np.ndarray, tile_size: int, overlap: i
     if world > 1:
         d.reduce(v, dst=0, group=group)
     return v.cpu().numpy() if rank == 0 else None
+
+
+def deconvolve_split(im: np.ndarray, psf: np.ndarray, group=None, **kw):
+    """One image split over the ranks of a process group, one GPU per rank
+    (dwcu_slab_part_*): rank r holds the z planes r, r + world, ... of the job
+    and the z-pass columns of its slab; the spectra are shared through CUDA
+    IPC handles (exchanged with all_gather_object), the ordering points are
+    stream-ordered all-reduces on the part's stream (NCCL) or host barriers
+    after a stream synchronisation (gloo), and the image sum and the
+    I-divergence sums are all-reduced.  Every rank passes the whole image
+    and PSF and gets the whole result (its own planes plus an all-reduce of
+    the others').  Without an initialised process group: one part in this
+    process (dwcu_deconvolve_slabs)."""
+    d = _dist()
+    if d is None:
+        return _core.run_slabs(im, psf, parts=1, **kw)
+    import torch
+    rank, world = d.get_rank(group), d.get_world_size(group)
+    dev = torch.cuda.current_device()
+    nccl = d.get_backend(group) == "nccl"
+    buf = torch.zeros(8, dtype=torch.float64, device=f"cuda:{dev}")
+    tok = torch.zeros(1, dtype=torch.float32, device=f"cuda:{dev}")
+
+    def barrier(stream):
+        ext = torch.cuda.ExternalStream(stream, device=dev)
+        if nccl:
+            with torch.cuda.stream(ext):
+                d.all_reduce(tok, group=group)
+        else:
+            ext.synchronize()
+            d.barrier(group=group)
+
+    def allreduce(stream, n, op):
+        ext = torch.cuda.ExternalStream(stream, device=dev)
+        rop = d.ReduceOp.SUM if op == 0 else d.ReduceOp.MIN
+        if nccl:
+            with torch.cuda.stream(ext):
+                d.all_reduce(buf[:n], op=rop, group=group)
+        else:
+            ext.synchronize()
+            t = buf[:n].cpu()
+            d.all_reduce(t, op=rop, group=group)
+            with torch.cuda.stream(ext):
+                buf[:n].copy_(t)
+            ext.synchronize()
+
+    part = _core.SlabPart(im.shape, psf.shape, world, rank, buf.data_ptr(), barrier, allreduce, device=dev, **kw)
+    try:
+        mine = part.export()
+        handles = [None] * world
+        d.all_gather_object(handles, mine, group=group)
+        for q in range(world):
+            if q != rank:
+                part.import_part(q, *handles[q])
+        out = np.zeros(im.shape, dtype=np.float32)
+        res = part.run(im, psf, out)
+    finally:
+        part.close()
+    # every plane comes from exactly one rank: the sum is the result
+    if nccl:
+        t = torch.from_numpy(out).to(f"cuda:{dev}")
+        d.all_reduce(t, group=group)
+        res.out = t.cpu().numpy()
+    else:
+        t = torch.from_numpy(out)
+        d.all_reduce(t, group=group)
+        res.out = t.numpy()
+    return res

@@ -134,6 +134,43 @@ int dwcu_deconvolve_slabs(const float *im, int64_t M, int64_t N, int64_t P,
 int dwcu_slab_layout(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP,
                      int32_t border_quality, int32_t nparts, int32_t part, int64_t info[6]);
 
+/* The same split with one process per part (a process per GPU, e.g. under
+ * torchrun): each process creates its part, exports the handle of its
+ * spectrum, imports every other part's (CUDA IPC), and runs.  The caller
+ * provides the collectives; every process calls them at the same points in
+ * the same order, with its part's stream:
+ *   barrier    work queued on `stream` before the call completes on every
+ *              part before work queued after it starts on any part (a
+ *              stream-ordered collective such as an NCCL all-reduce on that
+ *              stream, or a host barrier after synchronising the stream);
+ *   allreduce  the first n doubles of the sync buffer summed (op 0) or their
+ *              minimum taken (op 1) over the parts, in place, ordered the
+ *              same way.
+ * Both return 0 on success.  The plans are the recorded ones (an imported
+ * plan table, the same in every process) or the heuristic ones: no process
+ * measures plans of its own. */
+typedef struct dwcu_slab dwcu_slab;
+typedef struct dwcu_slab_sync {
+    int (*barrier)(void *ctx, void *stream);
+    int (*allreduce)(void *ctx, void *stream, int32_t n, int32_t op);
+    void *ctx;
+} dwcu_slab_sync;
+
+/* Part `part` of nparts on s->device; sync_buf: the caller's device buffer of
+ * at least 4 doubles (the allreduce's data). */
+int dwcu_slab_part_create(int64_t M, int64_t N, int64_t P, int64_t pM, int64_t pN, int64_t pP,
+                          const dwcu_opts *s, int32_t nparts, int32_t part, double *sync_buf,
+                          const dwcu_slab_sync *sync, dwcu_slab **out);
+/* The IPC handle (64 bytes) of the part's memory and its spectrum's offset in it. */
+int dwcu_slab_part_export(dwcu_slab *sl, void *handle, int64_t *offset);
+/* Map another part's spectrum from its exported handle and offset. */
+int dwcu_slab_part_import(dwcu_slab *sl, int32_t part, const void *handle, int64_t offset);
+/* Set-up, iterations and result: im and psf are the whole image and PSF (host);
+ * the part writes its own image planes z = l*nparts + part of `out` (host,
+ * M x N x P) and leaves the others untouched; s_out as dwcu_deconvolve's. */
+int dwcu_slab_part_run(dwcu_slab *sl, const float *im, const float *psf, float *out, dwcu_opts *s_out);
+void dwcu_slab_destroy(dwcu_slab *sl);
+
 /* ---------------------------------------------------------------- jobs */
 
 /* A job keeps its image, OTF, weights and estimates resident on the device
