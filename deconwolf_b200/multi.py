@@ -153,22 +153,11 @@ def deconvolve_tiled(im: np.ndarray, psf: np.ndarray, tile_size: int, overlap: i
     return v.cpu().numpy() if rank == 0 else None
 
 
-def deconvolve_split(im: np.ndarray, psf: np.ndarray, group=None, **kw):
-    """One image split over the ranks of a process group, one GPU per rank
-    (dwcu_slab_part_*): rank r holds the z planes r, r + world, ... of the job
-    and the z-pass columns of its slab; the spectra are shared through CUDA
-    IPC handles (exchanged with all_gather_object), the ordering points are
-    stream-ordered all-reduces on the part's stream (NCCL) or host barriers
-    after a stream synchronisation (gloo), and the image sum and the
-    I-divergence sums are all-reduced.  Every rank passes the whole image
-    and PSF and gets the whole result (its own planes plus an all-reduce of
-    the others').  Without an initialised process group: one part in this
-    process (dwcu_deconvolve_slabs)."""
-    d = _dist()
-    if d is None:
-        return _core.run_slabs(im, psf, parts=1, **kw)
+def _device_part(shape, psf_shape, world, rank, d, group, **kw):
+    """This rank's part on its GPU (dwcu_slab_part_*), with the collectives
+    the parts need: NCCL all-reduces on the part's stream, or (gloo) host
+    barriers after synchronising that stream."""
     import torch
-    rank, world = d.get_rank(group), d.get_world_size(group)
     dev = torch.cuda.current_device()
     nccl = d.get_backend(group) == "nccl"
     buf = torch.zeros(8, dtype=torch.float64, device=f"cuda:{dev}")
@@ -197,21 +186,45 @@ def deconvolve_split(im: np.ndarray, psf: np.ndarray, group=None, **kw):
                 buf[:n].copy_(t)
             ext.synchronize()
 
-    part = _core.SlabPart(im.shape, psf.shape, world, rank, buf.data_ptr(), barrier, allreduce, device=dev, **kw)
+    part = _core.SlabPart(shape, psf_shape, world, rank, buf.data_ptr(), barrier, allreduce, device=dev, **kw)
+    part._keep = (buf, tok)  # the buffers live as long as the part
+    return part
+
+
+def deconvolve_split(im: np.ndarray, psf: np.ndarray, group=None, part=None, **kw):
+    """One image split over the ranks of a process group, one GPU per rank
+    (dwcu_slab_part_*): rank r holds the z planes r, r + world, ... of the job
+    and the z-pass columns of its slab; the spectra are shared through CUDA
+    IPC handles (exchanged with all_gather_object), the ordering points are
+    stream-ordered all-reduces on the part's stream (NCCL) or host barriers
+    after a stream synchronisation (gloo), and the image sum and the
+    I-divergence sums are all-reduced.  Every rank passes the whole image
+    and PSF and gets the whole result (its own planes plus an all-reduce of
+    the others').  Without an initialised process group: one part in this
+    process (dwcu_deconvolve_slabs).  ``part``: a factory
+    ``part(shape, psf_shape, world, rank)`` of this rank's part (default: the
+    GPU part), so that the orchestration can run on CPU ranks."""
+    d = _dist()
+    if d is None:
+        return _core.run_slabs(im, psf, parts=1, **kw)
+    rank, world = d.get_rank(group), d.get_world_size(group)
+    p = (part(im.shape, psf.shape, world, rank) if part is not None
+         else _device_part(im.shape, psf.shape, world, rank, d, group, **kw))
     try:
-        mine = part.export()
+        mine = p.export()
         handles = [None] * world
         d.all_gather_object(handles, mine, group=group)
         for q in range(world):
             if q != rank:
-                part.import_part(q, *handles[q])
+                p.import_part(q, *handles[q])
         out = np.zeros(im.shape, dtype=np.float32)
-        res = part.run(im, psf, out)
+        res = p.run(im, psf, out)
     finally:
-        part.close()
+        p.close()
     # every plane comes from exactly one rank: the sum is the result
-    if nccl:
-        t = torch.from_numpy(out).to(f"cuda:{dev}")
+    import torch
+    if d.get_backend(group) == "nccl":
+        t = torch.from_numpy(out).to(f"cuda:{torch.cuda.current_device()}")
         d.all_reduce(t, group=group)
         res.out = t.cpu().numpy()
     else:

@@ -141,3 +141,67 @@ def test_two_ranks_match_one_process():
                 _oracle_runner(im[:4].copy(), psf[1:6], n_iter=2)]
     for a, b in zip(res, jobs_ref):
         np.testing.assert_array_equal(a, b)
+
+
+# ---------------------------------------------------------------- split over processes
+
+class _FakePart:
+    """Stands in for a rank's device part of a split job: its handle names
+    the rank, and its run writes the rank's planes (z = rank, rank + world,
+    ...) as twice the image."""
+
+    def __init__(self, shape, psf_shape, world, rank):
+        self.world, self.rank = world, rank
+        self.imported = {}
+        self.closed = False
+
+    def export(self):
+        return bytes([self.rank]) * 64, 1000 + self.rank
+
+    def import_part(self, q, handle, offset):
+        self.imported[q] = (handle[0], offset)
+
+    def run(self, im, psf, out):
+        out[self.rank::self.world] = 2 * im[self.rank::self.world]
+
+        class R:
+            pass
+        r = R()
+        r.out = out
+        return r
+
+    def close(self):
+        self.closed = True
+
+
+def _split_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        parts = []
+
+        def factory(shape, psf_shape, w, r):
+            parts.append(_FakePart(shape, psf_shape, w, r))
+            return parts[-1]
+
+        im = np.arange(7 * 5 * 4, dtype=np.float32).reshape(7, 5, 4)
+        res = multi.deconvolve_split(im, np.ones((3, 3, 3), np.float32), part=factory)
+        q.put((rank, parts[0].imported, parts[0].closed, res.out))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_over_ranks_exchanges_handles_and_combines_planes():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    mp.start_processes(_split_worker, args=(world, _free_port(), q), nprocs=world, join=True, start_method="spawn")
+    got = sorted(q.get() for _ in range(world))
+    im = np.arange(7 * 5 * 4, dtype=np.float32).reshape(7, 5, 4)
+    for rank, imported, closed, out in got:
+        others = [r for r in range(world) if r != rank]
+        assert imported == {r: (r, 1000 + r) for r in others}  # every other rank's handle and offset
+        assert closed
+        np.testing.assert_array_equal(out, 2 * im)  # every rank's planes, on every rank
