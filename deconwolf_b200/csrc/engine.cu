@@ -292,6 +292,7 @@ static long long x_blocks(const Geometry &g) { return g.Z * ((g.Y + g.xp->R - 1)
 struct DeviceCtx {
     int device = -1;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy = nullptr;  // image uploads that overlap a job's set-up passes
     std::map<long long, float2 *> tw;  // length -> exp(-2 pi i m / length)
 };
 
@@ -316,6 +317,7 @@ static int get_ctx(int device, DeviceCtx **out)
     auto *c = new DeviceCtx();
     c->device = device;
     CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
     g_ctx[device] = c;
     *out = c;
     return DWCU_SUCCESS;
@@ -1216,21 +1218,19 @@ static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_dev
     cudaStream_t st = j->stream;
     CU(cudaEventRecord(j->ev0, st));
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    CU(cudaMemcpy2DAsync(j->gimg, sizeof(float) * g.GP, im, sizeof(float) * g.M, sizeof(float) * g.M, g.N * g.P,
-                         kind, st));
+    // From host memory the image crosses PCIe on the device's copy stream
+    // while the OTF and the weights (which need only the image's size) are
+    // computed; the statistics wait for it (ev2 marks it; the result
+    // records ev2 again).  The PSF goes first: copies in one direction share
+    // one copy engine, and the OTF needs the PSF.
     const long long npsf = g.pM * g.pN * g.pP;
     CU(cudaMemcpyAsync(j->psf_dev, psf, sizeof(float) * npsf, kind, st));
     CU(cudaMemsetAsync(j->sc, 0, sizeof(JobScalars), st));
-
-    // background and start value
-    const long long nrows = g.N * g.P;
-    const long long rpb = (nrows + j->n_spart - 1) / j->n_spart;
-    const int nsb = (int) ((nrows + rpb - 1) / rpb);
-    k_stats_partial<<<nsb, kRedThreads, 0, st>>>(j->gimg, g.GP, (int) g.M, nrows, rpb, j->spart);
-    CHECK_LAUNCH();
-    k_stats_final<<<1, kRedThreads, 0, st>>>(j->spart, nsb, j->sc, j->s.bg_auto, j->s.bg,
-                                             (unsigned long long) (g.wM * g.wN * g.wP));
-    CHECK_LAUNCH();
+    cudaStream_t cs = on_device ? st : j->ctx->copy;
+    if (cs != st) CU(cudaStreamWaitEvent(cs, j->ev0, 0));
+    CU(cudaMemcpy2DAsync(j->gimg, sizeof(float) * g.GP, im, sizeof(float) * g.M, sizeof(float) * g.M, g.N * g.P,
+                         kind, cs));
+    if (cs != st) CU(cudaEventRecord(j->ev2, cs));
 
     // OTF: PSF with its first maximum at the origin, scaled by 1/(X*Y*Z)
     const long long per = (npsf + j->n_apart - 1) / j->n_apart;
@@ -1270,6 +1270,19 @@ static int job_setup(dwcu_job *j, const float *im, const float *psf, bool on_dev
         TRY(pass_x(j, XOP_FWD_ONES, 1, j->S, nullptr, nullptr, nullptr, 0, 0));
         TRY(conv(j, 1));
         TRY(pass_x(j, XOP_WEIGHTS, 0, j->S, nullptr, nullptr, j->W, 0, 0));
+    }
+
+    // background and start value (the image is on the device from here on)
+    if (cs != st) CU(cudaStreamWaitEvent(st, j->ev2, 0));
+    {
+        const long long nrows = g.N * g.P;
+        const long long rpb = (nrows + j->n_spart - 1) / j->n_spart;
+        const int nsb = (int) ((nrows + rpb - 1) / rpb);
+        k_stats_partial<<<nsb, kRedThreads, 0, st>>>(j->gimg, g.GP, (int) g.M, nrows, rpb, j->spart);
+        CHECK_LAUNCH();
+        k_stats_final<<<1, kRedThreads, 0, st>>>(j->spart, nsb, j->sc, j->s.bg_auto, j->s.bg,
+                                                 (unsigned long long) (g.wM * g.wN * g.wP));
+        CHECK_LAUNCH();
     }
 
     // start estimate (method_shb.c:264-276); x_{-1} = x_0
