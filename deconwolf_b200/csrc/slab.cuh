@@ -912,6 +912,9 @@ int dwcu_slab_part_run(dwcu_slab *sl, const float *im, const float *psf, float *
     if (!sl || !im || !psf || !out) return fail(DWCU_ERROR_INVALID_VALUE, "NULL argument");
     if (sl->local < 0) return fail(DWCU_ERROR_INVALID_VALUE, "not a part of a split over processes");
     if (sl->setup_done) return fail(DWCU_ERROR_INVALID_VALUE, "the part has run already");
+    for (size_t q = 0; q < sl->parts.size(); ++q)
+        if (!sl->parts[q].S)
+            return fail(DWCU_ERROR_INVALID_VALUE, "part %zu's spectrum is not mapped (dwcu_slab_part_import)", q);
     if (so) so->iterations_done = 0;
     int rc = slab_setup(sl, im, psf);
     if (rc == DWCU_SUCCESS) rc = slab_run(sl);
