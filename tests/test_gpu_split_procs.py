@@ -105,6 +105,16 @@ def test_two_processes_equal_one_process(tmp_path, case, env, heuristic_plans, m
     assert rel_l2(res[0]["out"], whole.out) < 1e-5
 
 
+def test_three_processes_equal_one_process(tmp_path, heuristic_plans):
+    case = dict(method="shb", n_iter=9, border_quality=1)
+    res = _run(tmp_path, 3, "gloo", {}, case)
+    im, psf = _inputs()
+    ref = dw.run_slabs(im, psf, parts=3, **case)
+    for r in res:
+        np.testing.assert_array_equal(r["out"], ref.out)
+        np.testing.assert_array_equal(r["trace"], ref.trace)
+
+
 def test_nccl_single_rank_equals_one_part(tmp_path, heuristic_plans):
     case = dict(method="shb", n_iter=10)
     res = _run(tmp_path, 1, "nccl", {}, case)
@@ -112,3 +122,15 @@ def test_nccl_single_rank_equals_one_part(tmp_path, heuristic_plans):
     ref = dw.run_slabs(im, psf, parts=1, **case)
     np.testing.assert_array_equal(res[0]["out"], ref.out)
     np.testing.assert_array_equal(res[0]["trace"], ref.trace)
+
+
+def test_run_before_every_part_is_mapped_is_refused():
+    import torch
+    im, psf = _inputs()
+    buf = torch.zeros(8, dtype=torch.float64, device="cuda")
+    part = dw.SlabPart(im.shape, psf.shape, 2, 0, buf.data_ptr(), lambda s: None, lambda s, n, op: None,
+                       method="shb", n_iter=3)
+    with pytest.raises(dw.DwcuError) as e:
+        part.run(im, psf, np.zeros(im.shape, np.float32))
+    assert e.value.code == 1  # DWCU_ERROR_INVALID_VALUE: part 1 was never imported
+    part.close()
