@@ -205,3 +205,59 @@ def test_split_over_ranks_exchanges_handles_and_combines_planes():
         assert imported == {r: (r, 1000 + r) for r in others}  # every other rank's handle and offset
         assert closed
         np.testing.assert_array_equal(out, 2 * im)  # every rank's planes, on every rank
+
+
+class _FailingPart(_FakePart):
+    def run(self, im, psf, out):
+        if self.rank == 1:
+            raise RuntimeError("part failed")
+        return super().run(im, psf, out)
+
+
+def _failing_worker(rank, world, port, q):
+    from datetime import timedelta
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=10))
+    outcome = "finished"
+    try:
+        im = np.zeros((6, 5, 4), np.float32)
+        multi.deconvolve_split(im, np.ones((3, 3, 3), np.float32),
+                               part=lambda shape, psf_shape, w, r: _FailingPart(shape, psf_shape, w, r))
+    except Exception as e:  # the failing part, or the peer's collective ending with an error
+        outcome = type(e).__name__ + ": " + str(e)[:60]
+    q.put((rank, outcome))
+    if rank == 1:
+        return  # leaves without the result's collective, as a crashed rank would
+    try:
+        dist.destroy_process_group()
+    except Exception:
+        pass
+
+
+def test_a_failing_rank_ends_the_split_on_every_rank():
+    """A rank whose part fails leaves the split; the other rank's next
+    collective ends with an error within the process group's timeout
+    instead of waiting for good."""
+    import time
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    t0 = time.time()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    alive = [p.is_alive() for p in procs]
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+            p.join()
+    assert not any(alive), "a rank waited for good"
+    got = dict(q.get() for _ in range(world))
+    assert got[1].startswith("RuntimeError: part failed")
+    assert got[0] != "finished"
+    assert time.time() - t0 < 120
